@@ -1,0 +1,349 @@
+"""Benchmark: RNS negacyclic NTT + INTT roundtrip at N = 2^16, 16 limbs.
+
+One step = forward then inverse transform (two launches, in place) over a
+batch of `--polys` polynomials of 2^16 x 16 uint32 limbs (4 MiB each; the
+default 64 polynomials = 256 MiB, larger than the 126 MB L2, so every step
+streams from HBM).  Moduli: the 16 ascending primes q == 1 mod 2^17 from
+974258177, smallest generators; coefficients uniform in [0, q) from seed
+1234.  Metric: limb-NTT/s, each limb forward or inverse transform counting
+one (whole job, all ranks).
+
+Launched with torchrun for N > 1: one rank per GPU, each transforming its
+own batch (limbs and polynomials are independent: weak scaling, no
+collective on the data path); time = max over ranks of the device-timed
+region.  `--impl reference` times the reference's CPU implementation of the
+same path (oracle/_ref: its unchanged cpu_ntt_butterfly /
+cpu_intt_butterfly, limbs split over all host threads) on rank 0 only.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LOGN, LIMBS, FIRST_Q, SEED = 16, 16, 974258177, 1234
+METRIC = "limb-NTT/s at 2^16x16 limbs"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--polys", type=int, default=64)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def moduli():
+    from oracle import oracle as O  # moduli search is host logic shared with the tests
+    return O.ascending_primes(LOGN, LIMBS, FIRST_Q)
+
+
+# ---------------------------------------------------------------------------
+# CPU reference / baseline
+# ---------------------------------------------------------------------------
+
+def cpu_roundtrip_rate(seconds, threads):
+    """Reference CPU path (oracle/_ref when built here, else the oracle port)
+    on one 2^16 x 16 polynomial per repetition, forward + inverse, limbs
+    split over `threads` host threads; repeated for about `seconds`."""
+    from oracle import oracle as O
+    mods = moduli()
+    T = O.LimbTables(LOGN, mods)
+    x = O.uniform_limbs(LOGN, T.q, SEED)
+    R = O.ref_lib()
+    kind = "reference" if R is not None else "port"
+    fn = R.ref_cpu_transform_limbs if R is not None else O.lib().oracle_transform_limbs
+    P = O._ptr
+    reps, t0 = 0, time.perf_counter()
+    a = x.copy()
+    while True:
+        fn(P(a), LOGN, LIMBS, P(T.q), P(T.psi_tab), None, threads)
+        fn(P(a), LOGN, LIMBS, P(T.q), P(T.inv_tab), P(T.degree_inv), threads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    if not np.array_equal(a, x):
+        raise RuntimeError("CPU reference roundtrip is not the identity")
+    return 2 * LIMBS * reps / el, kind, reps, el
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return  # other ranks exit 0 without work
+    threads = os.cpu_count() or 1
+    rates = []
+    for _ in range(max(args.warmup, 0)):
+        cpu_roundtrip_rate(0.0, threads)
+    t_total = time.perf_counter()
+    for _ in range(max(1, args.steps if args.steps <= 50 else 50)):
+        r, kind, reps, el = cpu_roundtrip_rate(0.0, threads)
+        rates.append(r)
+    total = time.perf_counter() - t_total
+    value = float(np.median(rates))
+    steps = len(rates)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "limb-NTT/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * total / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "NTT+INTT roundtrip, N=2^16, 16 limbs, 1 polynomial per step "
+                               "(CPU: one 4 MiB polynomial per step)",
+                   "moduli": f"16 ascending primes q=1 mod 2^17 from {FIRST_Q}", "seed": SEED},
+        "cpu_baseline": {"value": value, "unit": "limb-NTT/s", "cores": threads, "kind": kind,
+                         "sample": "one 2^16 x 16-limb polynomial forward+inverse per step"},
+        "e2e": {"value": value, "unit": "limb-NTT/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    import ntt_b200 as nb
+
+    mods = moduli()
+    plan = nb.Plan(LOGN, mods)
+    N = 1 << LOGN
+    P = args.polys
+    words = P * LIMBS * N
+    from oracle import oracle as O
+    q = np.array([m[0] for m in mods], dtype=np.uint64)
+    rng = np.random.default_rng(SEED + rank)
+    x = rng.integers(0, q[None, :, None], size=(P, LIMBS, N), dtype=np.uint64).astype(np.uint32)
+    host_in = torch.from_numpy(x.reshape(-1).view(np.int32)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    d = torch.empty(words, dtype=torch.int32, device="cuda")
+    d.copy_(host_in)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # correctness spot check of the timed path (limb 0 and 15 of polynomial 0)
+    with torch.cuda.stream(stream):
+        plan.forward_many(d, P, 0, stream=sh)
+    stream.synchronize()
+    T = O.LimbTables(LOGN, [mods[0], mods[15]])
+    got = d[: LIMBS * N].cpu().numpy().view(np.uint32).reshape(LIMBS, N)[[0, 15]]
+    if not np.array_equal(got, T.forward_mont(x[0][[0, 15]])):
+        raise RuntimeError("forward output differs from the oracle")
+    with torch.cuda.stream(stream):
+        plan.inverse_many(d, P, 0, stream=sh)
+    stream.synchronize()
+    if not torch.equal(d, host_in.cuda()):
+        raise RuntimeError("roundtrip is not the identity")
+
+    # warm-up
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            plan.forward_many(d, P, 0, stream=sh)
+            plan.inverse_many(d, P, 0, stream=sh)
+    barrier()
+
+    K = args.steps
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4 * K)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.25)
+    barrier()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        t_start.record(stream)
+        for k in range(K):
+            ev[4 * k].record(stream)
+            plan.forward_many(d, P, 0, stream=sh)
+            ev[4 * k + 1].record(stream)
+            ev[4 * k + 2].record(stream)
+            plan.inverse_many(d, P, 0, stream=sh)
+            ev[4 * k + 3].record(stream)
+        t_end.record(stream)
+    stream.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    elapsed_ms = t_start.elapsed_time(t_end)
+    fwd_ms = np.array([ev[4 * k].elapsed_time(ev[4 * k + 1]) for k in range(K)])
+    inv_ms = np.array([ev[4 * k + 2].elapsed_time(ev[4 * k + 3]) for k in range(K)])
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_max = float(t.item())
+
+    # e2e through the public API with host buffers (pinned), copies timed
+    E = max(1, args.e2e_steps)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(E):
+            d.copy_(host_in, non_blocking=True)
+            plan.forward_many(d, P, 0, stream=sh)
+            plan.inverse_many(d, P, 0, stream=sh)
+            host_out.copy_(d, non_blocking=True)
+        e1.record(stream)
+    stream.synchronize()
+    e2e_ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    if not torch.equal(host_out, host_in):
+        raise RuntimeError("e2e roundtrip is not the identity")
+
+    transforms = 2 * P * LIMBS * K * world
+    value = transforms / (elapsed_max / 1000.0)
+    e2e_value = 2 * P * LIMBS * E * world / (float(e2e_ms.item()) / 1000.0)
+
+    # roofline of the dominant kernel: algorithmic bytes = read + write of
+    # every word once per launch (8 bytes per coefficient)
+    alg_bytes = 8.0 * P * LIMBS * N
+    fwd_avg, inv_avg = float(fwd_ms.mean()), float(inv_ms.mean())
+    dom, dom_ms = ("forward", fwd_avg) if fwd_avg >= inv_avg else ("inverse", inv_avg)
+    achieved = alg_bytes / (dom_ms / 1000.0) / 1e9
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak, peak_src = json.load(open(peaks_path))["hbm_gbs"], "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        tj = json.load(open(tpath))
+        per = tj.get(dom)
+        if per:
+            traffic = per["bytes_per_coefficient"] * P * LIMBS * N
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "limb-NTT/s", "n_gpus": world,
+        "steps": K, "warmup": args.warmup, "ms_per_step": elapsed_max / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic",
+        "config": {"workload": f"NTT+INTT roundtrip, N=2^16, 16 limbs, {P} polynomials per "
+                               "rank per step (in place, one launch per direction)",
+                   "moduli": f"16 ascending primes q=1 mod 2^17 from {FIRST_Q}",
+                   "seed": SEED, "parallelism": f"dp{world} (independent polynomials)",
+                   "l2": f"inputs {P * LIMBS * N * 4 >> 20} MiB per rank > 126 MB L2, "
+                         "no flush needed"},
+        "e2e": {"value": e2e_value, "unit": "limb-NTT/s",
+                "h2d_bytes_per_step": P * LIMBS * N * 4, "d2h_bytes_per_step": P * LIMBS * N * 4,
+                "steps": E},
+        "gpu_launches": 2 * K,
+        "roofline": {"bound": "hbm", "kernel": f"fused_kernel ({dom})", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "forward_ms": fwd_avg, "inverse_ms": inv_avg},
+        "clocks": clocks,
+    }
+    info = plan.info
+    out["config"]["kernel"] = {"cluster_ctas": info.cluster_ctas,
+                               "threads_per_cta": info.threads_per_cta,
+                               "smem_bytes": info.smem_bytes,
+                               "phases": [info.effective.ntt_phase1.as_tuple(),
+                                          info.effective.ntt_phase2.as_tuple()]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, kind, reps, el = cpu_roundtrip_rate(args.cpu_seconds, threads)
+        out["cpu_baseline"] = {"value": rate, "unit": "limb-NTT/s", "cores": threads,
+                               "kind": kind,
+                               "sample": f"{reps} forward+inverse roundtrips of one 2^16 x 16 "
+                                         f"polynomial in {el:.1f} s"}
+    if rank == 0:
+        print(json.dumps(out))
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

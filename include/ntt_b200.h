@@ -1,0 +1,181 @@
+/*
+ * ntt_b200 -- RNS negacyclic NTT / INTT for NVIDIA B200 (sm_100a).
+ *
+ * C ABI of libntt_b200.so.  Plain pointers and sizes only; device pointers
+ * are CUDA device addresses, streams are cudaStream_t passed as void*.
+ * Every entry point returns an ntt_status_t (never exits the process);
+ * ntt_last_error() gives the calling thread's detail string.
+ *
+ * Reference interfaces replaced (vnny27/NTT):
+ *   src/ntt_config.h:6-29     ModulusConfig / PhaseConfig / TransformConfig
+ *   src/v04_montgomery.cu:17-26    ModulusRuntime
+ *   src/v04_montgomery.cu:660-740  host precompute (make_modulus_runtime,
+ *                                  make_twiddle_table, to_mont, ...)
+ *   src/v04_montgomery.cu:603-658  launch_ntt<LC> / launch_intt<LC>
+ * The C++ drop-in spellings of the templates (DefaultNTTLaunchConfig<LogN>,
+ * launch_ntt<LC>, ...) are in ntt_b200_config.hpp.
+ *
+ * Domain contract (identical to the reference's v04 path):
+ *   forward: normal-domain input (any uint32, reduced mod q) -> Montgomery
+ *            domain output (x * 2^32 mod q), bit-reversed order, in [0, q);
+ *   inverse: Montgomery-domain input in [0, q), bit-reversed order ->
+ *            normal-domain output in natural order, N^{-1} applied;
+ *   layout:  limb-major, A[limb * N + i], in place.
+ */
+#ifndef NTT_B200_H
+#define NTT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define NTT_API __attribute__((visibility("default")))
+#else
+#define NTT_API
+#endif
+
+#define NTT_B200_VERSION 100 /* 1.0.0 */
+#define NTT_MIN_LOGN 1
+#define NTT_MAX_LOGN 17
+
+/* src/ntt_config.h:6-9 */
+typedef struct ModulusConfig {
+    uint32_t qi;
+    uint32_t primitive_root;
+} ModulusConfig;
+
+/* src/ntt_config.h:12-16 (all log2 values) */
+typedef struct PhaseConfig {
+    int radix_stages;  /* radix-2 stages handled by this phase            */
+    int stage_merging; /* stages merged in one register pass (max)        */
+    int warp_batching; /* log2 contiguous words per thread at phase I/O  */
+} PhaseConfig;
+
+/* src/ntt_config.h:18-23 */
+typedef struct TransformConfig {
+    PhaseConfig ntt_phase1;
+    PhaseConfig ntt_phase2;
+    PhaseConfig intt_phase1;
+    PhaseConfig intt_phase2;
+} TransformConfig;
+
+/* src/v04_montgomery.cu:17-26 */
+typedef struct ModulusRuntime {
+    uint32_t qi;
+    uint32_t primitive_root;
+    uint32_t q_inv;   /* -q^{-1} mod 2^32                 */
+    uint32_t r2;      /* 2^64 mod q                       */
+    uint32_t psi;     /* primitive 2N-th root of unity    */
+    uint32_t psi_inv;
+    uint32_t omega;   /* psi^2                            */
+    uint32_t degree_inv; /* N^{-1} mod q (normal domain)  */
+} ModulusRuntime;
+
+typedef enum ntt_status {
+    NTT_OK = 0,
+    NTT_ERR_INVALID_ARGUMENT = 1,
+    NTT_ERR_MODULUS = 2,          /* q != 1 mod 2N      (reference: exit, v04:685-689) */
+    NTT_ERR_ROOT = 3,             /* not a 2N-th root   (reference: exit, v04:703-707) */
+    NTT_ERR_MODULUS_RANGE = 4,    /* q even, composite, or >= 2^31                       */
+    NTT_ERR_UNSUPPORTED = 5,      /* logN outside [NTT_MIN_LOGN, NTT_MAX_LOGN]           */
+    NTT_ERR_MISALIGNED = 6,       /* device pointer not 16-byte aligned                  */
+    NTT_ERR_CUDA = 7,             /* a CUDA runtime call failed (see ntt_last_error)    */
+    NTT_ERR_OUT_OF_MEMORY = 8,
+    NTT_ERR_BUDGET = 9,           /* request does not fit the server's memory budget    */
+    NTT_ERR_TIMEOUT = 10,         /* bounded wait expired                               */
+    NTT_ERR_CANCELLED = 11,
+    NTT_ERR_NOT_READY = 12,
+    NTT_ERR_SHUTDOWN = 13
+} ntt_status_t;
+
+typedef struct ntt_plan ntt_plan_t;
+typedef void* ntt_stream_t; /* cudaStream_t; NULL = legacy default stream */
+
+NTT_API int ntt_version(void);
+NTT_API const char* ntt_status_string(ntt_status_t status);
+/* Detail of the calling thread's most recent failure ("" if none). */
+NTT_API const char* ntt_last_error(void);
+
+/* ---- host precompute (mirrors of src/v04_montgomery.cu:660-740) -------- */
+
+/* make_modulus_runtime (v04:681-718) with status codes instead of exit. */
+NTT_API ntt_status_t ntt_modulus_runtime(int logN, ModulusConfig cfg, ModulusRuntime* out);
+/* make_twiddle_table (v04:720-727): out[i] = root^bitrev(i, logN) mod q,
+ * out must hold 2^logN words (host memory). */
+NTT_API ntt_status_t ntt_twiddle_table_host(int logN, uint32_t q, uint32_t root, uint32_t* out);
+/* default_moduli() (src/ntt_config.h:75-94): writes min(cap, 16) entries,
+ * returns 16. */
+NTT_API int ntt_default_moduli(ModulusConfig* out, int cap);
+/* DefaultNTTLaunchConfig<LogN>::runtime_transform() (src/ntt_config.h:62-73). */
+NTT_API ntt_status_t ntt_default_transform(int logN, TransformConfig* out);
+/* The first `count` primes q >= lower_bound with q == 1 (mod 2N), ascending,
+ * each with its smallest primitive root (no reference counterpart: the
+ * reference hard-codes its moduli). */
+NTT_API ntt_status_t ntt_find_moduli(int logN, int count, uint32_t lower_bound, ModulusConfig* out);
+
+/* ---- plans ------------------------------------------------------------ */
+
+typedef struct ntt_plan_info {
+    int logN;
+    int limbs;
+    int cluster_ctas;       /* CTAs cooperating on one limb (DSMEM cluster)  */
+    int threads_per_cta;
+    uint32_t smem_bytes;    /* dynamic shared memory per CTA                */
+    TransformConfig effective; /* the phase triples the kernels run          */
+    size_t device_bytes;    /* twiddle tables + constants held by the plan  */
+    int tuned;              /* 1 if the configuration came from the tuner   */
+} ntt_plan_info_t;
+
+/* Validates every (qi, primitive_root) exactly as make_modulus_runtime does
+ * (plus q odd, prime and < 2^31), then builds device-resident Shoup twiddle
+ * tables on the current CUDA device with a generation kernel.
+ * transform: NULL = tuned or default configuration; otherwise its phase
+ * split (radix_stages) must add up to logN and selects among the compiled
+ * kernel configurations (results do not depend on it). */
+NTT_API ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int limbs,
+                             const TransformConfig* transform, ntt_plan_t** out);
+NTT_API ntt_status_t ntt_plan_destroy(ntt_plan_t* plan);
+NTT_API ntt_status_t ntt_plan_get_info(const ntt_plan_t* plan, ntt_plan_info_t* out);
+/* Device pointers of the plan's tables: limbs * N (w, w') uint32 pairs, with
+ * entries 0 and 1 holding the constants folded into limb stage 0. */
+NTT_API ntt_status_t ntt_plan_tables(const ntt_plan_t* plan, const uint32_t** fwd_pairs,
+                             const uint32_t** inv_pairs, const uint32_t** moduli);
+
+/* In-place transforms of one polynomial (limbs * N words, 16-byte aligned). */
+NTT_API ntt_status_t ntt_forward(const ntt_plan_t* plan, uint32_t* a_dev, ntt_stream_t stream);
+NTT_API ntt_status_t ntt_inverse(const ntt_plan_t* plan, uint32_t* a_dev, ntt_stream_t stream);
+/* `polys` polynomials, polynomial p at a_dev + p * poly_stride (words,
+ * >= limbs * N, multiple of 4); one launch. */
+NTT_API ntt_status_t ntt_forward_many(const ntt_plan_t* plan, uint32_t* a_dev, size_t polys,
+                              size_t poly_stride, ntt_stream_t stream);
+NTT_API ntt_status_t ntt_inverse_many(const ntt_plan_t* plan, uint32_t* a_dev, size_t polys,
+                              size_t poly_stride, ntt_stream_t stream);
+
+/* ---- drop-in launchers (src/v04_montgomery.cu:603-658) -----------------
+ * Same arguments and domain contract as launch_ntt<LC> / launch_intt<LC>:
+ * caller-owned device buffers, the reference's Montgomery-form tables
+ * (twiddle_dev[limb*N + i] = to_mont(psi^bitrev(i))), launched on the legacy
+ * default stream.  phase1/phase2: the LC's NTT (or INTT) phase triples, or
+ * NULL for DefaultNTTLaunchConfig<logN>.  On first use of a given set of
+ * table pointers the tables are converted once on the device into Shoup form
+ * and cached (so the caller's tables must stay unchanged while in use; see
+ * ntt_shim_cache_clear).  Unlike the reference, errors are returned. */
+NTT_API ntt_status_t ntt_launch_ntt(uint32_t* A_dev, const uint32_t* twiddle_dev,
+                            const uint32_t* moduli_dev, const uint32_t* q_inv_dev,
+                            const uint32_t* r2_dev, size_t limb_count, int logN,
+                            const PhaseConfig* phase1, const PhaseConfig* phase2);
+NTT_API ntt_status_t ntt_launch_intt(uint32_t* A_dev, const uint32_t* inv_twiddle_dev,
+                             const uint32_t* moduli_dev, const uint32_t* q_inv_dev,
+                             const uint32_t* degree_inv_dev, size_t limb_count, int logN,
+                             const PhaseConfig* phase1, const PhaseConfig* phase2);
+/* Frees the converted tables cached by the drop-in launchers. */
+NTT_API void ntt_shim_cache_clear(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NTT_B200_H */

@@ -1,0 +1,379 @@
+"""ntt_b200 -- RNS negacyclic NTT / INTT on NVIDIA B200 (sm_100a).
+
+Python host side over the C ABI of ``libntt_b200.so`` (include/ntt_b200.h).
+It mirrors the reference's interface for this path (vnny27/NTT):
+
+* ``ModulusConfig``, ``PhaseConfig``, ``TransformConfig`` -- src/ntt_config.h:6-29
+* ``default_moduli()``, ``default_transform(logN)`` -- src/ntt_config.h:62-94
+* ``modulus_runtime(logN, cfg)`` -- make_modulus_runtime, src/v04_montgomery.cu:681-718
+* ``twiddle_table(logN, q, root)`` -- make_twiddle_table, v04:720-727
+* ``launch_ntt(...)`` / ``launch_intt(...)`` -- launch_ntt<LC> / launch_intt<LC>,
+  v04:603-658 (same arguments: caller-owned device buffers and the reference's
+  Montgomery-form tables)
+
+plus the native ``Plan`` (device-resident Shoup tables, fused cluster
+kernels), the batch / multiply / serving layers and the autotuner.
+
+Device buffers can be passed as torch CUDA tensors (int32 or uint32) or raw
+integer device addresses; streams as ``torch.cuda.Stream``, raw handles or
+None (legacy default stream).  There is no CPU fallback: every call goes
+through the compiled library, and importing fails loudly if it is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Iterable, List, Optional, Sequence
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libntt_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"ntt_b200: compiled library {LIB_PATH} is missing; build it with "
+        "`make -C ntt_b200` (or __graft_entry__.build())")
+
+_lib = ctypes.CDLL(LIB_PATH)
+
+# ---------------------------------------------------------------------------
+# C types
+# ---------------------------------------------------------------------------
+
+
+class ModulusConfig(ctypes.Structure):
+    """src/ntt_config.h:6-9"""
+    _fields_ = [("qi", ctypes.c_uint32), ("primitive_root", ctypes.c_uint32)]
+
+    def __iter__(self):
+        yield self.qi
+        yield self.primitive_root
+
+    def __repr__(self):
+        return f"ModulusConfig({self.qi}, {self.primitive_root})"
+
+
+class PhaseConfig(ctypes.Structure):
+    """src/ntt_config.h:12-16"""
+    _fields_ = [("radix_stages", ctypes.c_int), ("stage_merging", ctypes.c_int),
+                ("warp_batching", ctypes.c_int)]
+
+    def as_tuple(self):
+        return (self.radix_stages, self.stage_merging, self.warp_batching)
+
+    def __repr__(self):
+        return f"PhaseConfig{self.as_tuple()}"
+
+
+class TransformConfig(ctypes.Structure):
+    """src/ntt_config.h:18-23"""
+    _fields_ = [("ntt_phase1", PhaseConfig), ("ntt_phase2", PhaseConfig),
+                ("intt_phase1", PhaseConfig), ("intt_phase2", PhaseConfig)]
+
+
+class ModulusRuntime(ctypes.Structure):
+    """src/v04_montgomery.cu:17-26"""
+    _fields_ = [(n, ctypes.c_uint32) for n in (
+        "qi", "primitive_root", "q_inv", "r2", "psi", "psi_inv", "omega", "degree_inv")]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("logN", ctypes.c_int), ("limbs", ctypes.c_int), ("cluster_ctas", ctypes.c_int),
+                ("threads_per_cta", ctypes.c_int), ("smem_bytes", ctypes.c_uint32),
+                ("effective", TransformConfig), ("device_bytes", ctypes.c_size_t),
+                ("tuned", ctypes.c_int)]
+
+
+class KernelConfig(ctypes.Structure):
+    _fields_ = [("logN", ctypes.c_int), ("cluster_ctas", ctypes.c_int), ("r1", ctypes.c_int),
+                ("words_log2", ctypes.c_int), ("k1a", ctypes.c_int), ("k2a", ctypes.c_int),
+                ("threads", ctypes.c_int), ("smem_bytes", ctypes.c_uint32)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("config_index", ctypes.c_int), ("roundtrip_us", ctypes.c_double),
+                ("candidates", ctypes.c_int)]
+
+
+NTT_OK = 0
+STATUS_NAMES = {
+    0: "NTT_OK", 1: "NTT_ERR_INVALID_ARGUMENT", 2: "NTT_ERR_MODULUS", 3: "NTT_ERR_ROOT",
+    4: "NTT_ERR_MODULUS_RANGE", 5: "NTT_ERR_UNSUPPORTED", 6: "NTT_ERR_MISALIGNED",
+    7: "NTT_ERR_CUDA", 8: "NTT_ERR_OUT_OF_MEMORY", 9: "NTT_ERR_BUDGET", 10: "NTT_ERR_TIMEOUT",
+    11: "NTT_ERR_CANCELLED", 12: "NTT_ERR_NOT_READY", 13: "NTT_ERR_SHUTDOWN",
+}
+
+
+class NttError(RuntimeError):
+    """A non-OK ntt_status_t.  ``status`` is the numeric code, ``name`` its
+    enumerator name."""
+
+    def __init__(self, status: int, where: str):
+        self.status = int(status)
+        self.name = STATUS_NAMES.get(self.status, str(status))
+        detail = _lib.ntt_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {self.name}: {detail}")
+
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_vp = ctypes.c_void_p
+_st = ctypes.c_int
+
+
+def _sig(name, res, *args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_sig("ntt_version", ctypes.c_int)
+_sig("ntt_status_string", ctypes.c_char_p, _st)
+_sig("ntt_last_error", ctypes.c_char_p)
+_sig("ntt_modulus_runtime", _st, ctypes.c_int, ModulusConfig, ctypes.POINTER(ModulusRuntime))
+_sig("ntt_twiddle_table_host", _st, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp)
+_sig("ntt_default_moduli", ctypes.c_int, ctypes.POINTER(ModulusConfig), ctypes.c_int)
+_sig("ntt_default_transform", _st, ctypes.c_int, ctypes.POINTER(TransformConfig))
+_sig("ntt_find_moduli", _st, ctypes.c_int, ctypes.c_int, ctypes.c_uint32,
+     ctypes.POINTER(ModulusConfig))
+_sig("ntt_plan_create", _st, ctypes.c_int, ctypes.POINTER(ModulusConfig), ctypes.c_int,
+     ctypes.POINTER(TransformConfig), ctypes.POINTER(_vp))
+_sig("ntt_plan_destroy", _st, _vp)
+_sig("ntt_plan_get_info", _st, _vp, ctypes.POINTER(PlanInfo))
+_sig("ntt_plan_tables", _st, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp))
+_sig("ntt_forward", _st, _vp, _vp, _vp)
+_sig("ntt_inverse", _st, _vp, _vp, _vp)
+_sig("ntt_forward_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
+_sig("ntt_inverse_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
+_sig("ntt_launch_ntt", _st, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_int,
+     ctypes.POINTER(PhaseConfig), ctypes.POINTER(PhaseConfig))
+_sig("ntt_launch_intt", _st, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_int,
+     ctypes.POINTER(PhaseConfig), ctypes.POINTER(PhaseConfig))
+_sig("ntt_shim_cache_clear", None)
+_sig("ntt_config_count", ctypes.c_int)
+_sig("ntt_config_get", _st, ctypes.c_int, ctypes.POINTER(KernelConfig))
+_sig("ntt_autotune", _st, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+     ctypes.POINTER(TuneResult))
+_sig("ntt_autotune_forget", None)
+_sig("ntt_plan_force_config", _st, _vp, ctypes.c_int, ctypes.c_int)
+_sig("ntt_autotune_reload", None)
+
+
+def _check(st: int, where: str):
+    if st != NTT_OK:
+        raise NttError(st, where)
+
+
+def _ptr(x) -> Optional[int]:
+    """Device address of a torch tensor / raw int / None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if hasattr(x, "is_cuda") and not x.is_cuda:
+            raise ValueError("expected a CUDA tensor")
+        return int(x.data_ptr())
+    raise TypeError(f"cannot take a device pointer of {type(x)!r}")
+
+
+def _stream(s) -> Optional[int]:
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return s
+    if hasattr(s, "cuda_stream"):
+        return int(s.cuda_stream)
+    raise TypeError(f"cannot take a CUDA stream handle of {type(s)!r}")
+
+
+def version() -> int:
+    return _lib.ntt_version()
+
+
+# ---------------------------------------------------------------------------
+# host precompute (reference mirrors)
+# ---------------------------------------------------------------------------
+
+
+def _moduli_array(moduli: Iterable) -> "ctypes.Array":
+    ms = [m if isinstance(m, ModulusConfig) else ModulusConfig(int(m[0]), int(m[1]))
+          for m in moduli]
+    arr = (ModulusConfig * max(1, len(ms)))(*ms)
+    return arr, len(ms)
+
+
+def default_moduli() -> List[ModulusConfig]:
+    """default_moduli() -- src/ntt_config.h:75-94."""
+    n = _lib.ntt_default_moduli(None, 0)
+    arr = (ModulusConfig * n)()
+    _lib.ntt_default_moduli(arr, n)
+    return list(arr)
+
+
+def default_transform(logN: int) -> TransformConfig:
+    """DefaultNTTLaunchConfig<LogN>::runtime_transform() -- src/ntt_config.h:62-73."""
+    t = TransformConfig()
+    _check(_lib.ntt_default_transform(logN, ctypes.byref(t)), "default_transform")
+    return t
+
+
+def modulus_runtime(logN: int, cfg) -> ModulusRuntime:
+    """make_modulus_runtime -- raises NttError(NTT_ERR_MODULUS / NTT_ERR_ROOT)
+    where the reference calls std::exit."""
+    out = ModulusRuntime()
+    m = cfg if isinstance(cfg, ModulusConfig) else ModulusConfig(int(cfg[0]), int(cfg[1]))
+    _check(_lib.ntt_modulus_runtime(logN, m, ctypes.byref(out)), "modulus_runtime")
+    return out
+
+
+def twiddle_table(logN: int, q: int, root: int):
+    """make_twiddle_table: root^bitrev(i) mod q (host, numpy uint32)."""
+    import numpy as np
+    out = np.empty(1 << logN, dtype=np.uint32)
+    _check(_lib.ntt_twiddle_table_host(logN, q, root, out.ctypes.data), "twiddle_table")
+    return out
+
+
+def find_moduli(logN: int, count: int, lower_bound: int) -> List[ModulusConfig]:
+    """First `count` primes >= lower_bound with q == 1 (mod 2N), ascending,
+    with their smallest primitive roots."""
+    arr = (ModulusConfig * max(1, count))()
+    _check(_lib.ntt_find_moduli(logN, count, lower_bound, arr), "find_moduli")
+    return list(arr)[:count]
+
+
+# ---------------------------------------------------------------------------
+# plans
+# ---------------------------------------------------------------------------
+
+
+class Plan:
+    """Validated moduli + device-resident twiddle tables for one (logN,
+    modulus chain).  Immutable after creation; usable from several host
+    threads on different streams."""
+
+    def __init__(self, logN: int, moduli: Sequence, transform: Optional[TransformConfig] = None):
+        arr, n = _moduli_array(moduli)
+        h = _vp()
+        _check(_lib.ntt_plan_create(logN, arr, n,
+                                    ctypes.byref(transform) if transform is not None else None,
+                                    ctypes.byref(h)), "ntt_plan_create")
+        self._h = h
+        self.logN = logN
+        self.N = 1 << logN
+        self.limbs = n
+        self.moduli = [(m.qi, m.primitive_root) for m in arr[:n]]
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.ntt_plan_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def info(self) -> PlanInfo:
+        i = PlanInfo()
+        _check(_lib.ntt_plan_get_info(self._h, ctypes.byref(i)), "ntt_plan_get_info")
+        return i
+
+    def force_config(self, fwd_index: int = -1, inv_index: int = -1):
+        """Pin the plan to compiled configurations (see kernel_configs())."""
+        _check(_lib.ntt_plan_force_config(self._h, fwd_index, inv_index), "ntt_plan_force_config")
+
+    def tables(self):
+        """(forward pairs, inverse pairs, moduli) device addresses."""
+        f, i, q = _vp(), _vp(), _vp()
+        _check(_lib.ntt_plan_tables(self._h, ctypes.byref(f), ctypes.byref(i), ctypes.byref(q)),
+               "ntt_plan_tables")
+        return f.value, i.value, q.value
+
+    def forward(self, a, stream=None):
+        _check(_lib.ntt_forward(self._h, _ptr(a), _stream(stream)), "ntt_forward")
+
+    def inverse(self, a, stream=None):
+        _check(_lib.ntt_inverse(self._h, _ptr(a), _stream(stream)), "ntt_inverse")
+
+    def forward_many(self, a, polys: int, poly_stride: int = 0, stream=None):
+        _check(_lib.ntt_forward_many(self._h, _ptr(a), polys, poly_stride, _stream(stream)),
+               "ntt_forward_many")
+
+    def inverse_many(self, a, polys: int, poly_stride: int = 0, stream=None):
+        _check(_lib.ntt_inverse_many(self._h, _ptr(a), polys, poly_stride, _stream(stream)),
+               "ntt_inverse_many")
+
+
+# ---------------------------------------------------------------------------
+# drop-in launchers (v04:603-658)
+# ---------------------------------------------------------------------------
+
+
+def _phase(p):
+    if p is None:
+        return None
+    if isinstance(p, PhaseConfig):
+        return ctypes.byref(p)
+    return ctypes.byref(PhaseConfig(*p))
+
+
+def launch_ntt(A_dev, twiddle_dev, moduli_dev, q_inv_dev, r2_dev, limb_count: int, logN: int,
+               phase1=None, phase2=None):
+    """launch_ntt<LC>(A, tw, moduli, q_inv, r2, limb_count) with LC's logN and
+    NTT phase triples (None: DefaultNTTLaunchConfig<logN>)."""
+    _check(_lib.ntt_launch_ntt(_ptr(A_dev), _ptr(twiddle_dev), _ptr(moduli_dev), _ptr(q_inv_dev),
+                               _ptr(r2_dev), limb_count, logN, _phase(phase1), _phase(phase2)),
+           "ntt_launch_ntt")
+
+
+def launch_intt(A_dev, inv_twiddle_dev, moduli_dev, q_inv_dev, degree_inv_dev, limb_count: int,
+                logN: int, phase1=None, phase2=None):
+    """launch_intt<LC>(A, inv_tw, moduli, q_inv, degree_inv, limb_count)."""
+    _check(_lib.ntt_launch_intt(_ptr(A_dev), _ptr(inv_twiddle_dev), _ptr(moduli_dev),
+                                _ptr(q_inv_dev), _ptr(degree_inv_dev), limb_count, logN,
+                                _phase(phase1), _phase(phase2)), "ntt_launch_intt")
+
+
+def shim_cache_clear():
+    _lib.ntt_shim_cache_clear()
+
+
+# ---------------------------------------------------------------------------
+# configuration catalogue and autotuner
+# ---------------------------------------------------------------------------
+
+
+def kernel_configs() -> List[KernelConfig]:
+    out = []
+    for i in range(_lib.ntt_config_count()):
+        c = KernelConfig()
+        _check(_lib.ntt_config_get(i, ctypes.byref(c)), "ntt_config_get")
+        out.append(c)
+    return out
+
+
+def autotune(logN: int, limbs: int, polys: int = 8, iters: int = 5) -> TuneResult:
+    r = TuneResult()
+    _check(_lib.ntt_autotune(logN, limbs, polys, iters, ctypes.byref(r)), "ntt_autotune")
+    return r
+
+
+def autotune_forget():
+    _lib.ntt_autotune_forget()
+
+
+def autotune_reload():
+    _lib.ntt_autotune_reload()

@@ -1,0 +1,580 @@
+// Host runtime and C ABI of libntt_b200.so (see include/ntt_b200.h).
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <set>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/ntt_b200.h"
+#include "../../include/ntt_b200_tune.h"
+#include "configs.h"
+#include "fused_kernel.cuh"
+#include "host_math.h"
+#include "runtime.h"
+#include "small.h"
+#include "twiddle.h"
+
+using namespace nttb;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+namespace {
+thread_local std::string t_err;
+}
+
+namespace nttb {
+ntt_status_t fail(ntt_status_t st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_err = buf;
+    return st;
+}
+ntt_status_t cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? NTT_ERR_OUT_OF_MEMORY : NTT_ERR_CUDA,
+                "%s: %s", what, cudaGetErrorString(e));
+}
+}  // namespace nttb
+
+#define NTT_CUDA_TRY(call, what)                      \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// configuration registry helpers
+// ---------------------------------------------------------------------------
+namespace nttb {
+
+const FusedConfig* default_config(int logN) {
+    const FusedConfig* c = fused_configs();
+    for (int i = 0; i < fused_config_count(); ++i)
+        if (c[i].logN == logN) return &c[i];
+    return nullptr;
+}
+
+const FusedConfig* config_by_r1(int logN, int r1) {
+    const FusedConfig* c = fused_configs();
+    for (int i = 0; i < fused_config_count(); ++i)
+        if (c[i].logN == logN && c[i].r1 == r1) return &c[i];
+    return nullptr;
+}
+
+const FusedConfig* config_by_index(int idx) {
+    if (idx < 0 || idx >= fused_config_count()) return nullptr;
+    return &fused_configs()[idx];
+}
+
+// Phase triples (radix_stages, stage_merging, warp_batching) a fused
+// configuration actually runs.  warp_batching reports log2 of the run of
+// consecutive words each thread moves at the phase's global-memory side.
+void effective_triples(const FusedConfig* c, int logN, TransformConfig* t) {
+    if (!c) {  // single-CTA stage-per-round kernel
+        PhaseConfig p{logN, 1, 0};
+        *t = TransformConfig{p, PhaseConfig{0, 0, 0}, PhaseConfig{0, 0, 0}, p};
+        return;
+    }
+    const int r2 = logN - c->r1;
+    const int k1b = c->r1 - c->k1a, k2b = r2 - c->k2a;
+    const int s1 = r2 - c->clog;
+    int run1 = c->eb - c->k1a;
+    if (run1 > s1) run1 = s1;
+    PhaseConfig p1{c->r1, c->k1a > k1b ? c->k1a : k1b, run1};
+    PhaseConfig p2{r2, c->k2a > k2b ? c->k2a : k2b, c->eb};
+    *t = TransformConfig{p1, p2, p2, p1};
+}
+
+static std::mutex g_attr_mu;
+static std::set<std::pair<int, const void*>> g_attr_done;
+
+ntt_status_t prepare_function(const FusedConfig* c, const void* fn) {
+    int dev = 0;
+    NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    if (g_attr_done.count({dev, fn})) return NTT_OK;
+    if (c->smem_bytes > 48 * 1024)
+        NTT_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)c->smem_bytes),
+                     "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
+    if ((1 << c->clog) > 8)
+        NTT_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+                     "cudaFuncSetAttribute(NonPortableClusterSizeAllowed)");
+    g_attr_done.insert({dev, fn});
+    return NTT_OK;
+}
+
+ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s) {
+    if (a.jobs == 0) return NTT_OK;
+    const void* fn = fwd ? c->fwd : c->inv;
+    ntt_status_t st = prepare_function(c, fn);
+    if (st != NTT_OK) return st;
+    const unsigned C = 1u << c->clog;
+    if ((unsigned long long)a.jobs * C > (unsigned long long)INT_MAX)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "too many limb transforms in one launch");
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(C * a.jobs, 1, 1);
+    lc.blockDim = dim3((unsigned)c->threads, 1, 1);
+    lc.dynamicSmemBytes = c->smem_bytes;
+    lc.stream = s;
+    cudaLaunchAttribute attr[1];
+    if (C > 1) {
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+    }
+    FusedArgs arg = a;
+    void* args[] = {&arg};
+    NTT_CUDA_TRY(cudaLaunchKernelExC(&lc, fn, args), "fused NTT launch");
+    return NTT_OK;
+}
+
+}  // namespace nttb
+
+// ---------------------------------------------------------------------------
+// plans
+// ---------------------------------------------------------------------------
+struct ntt_plan {
+    int logN = 0, limbs = 0, device = 0;
+    std::vector<ModulusConfig> moduli;
+    void* block = nullptr;  // one allocation: fwd | inv | q
+    TwPair* fwd = nullptr;
+    TwPair* inv = nullptr;
+    uint32_t* q = nullptr;
+    size_t bytes = 0;
+    const FusedConfig* cfg_fwd = nullptr;  // nullptr: small kernel
+    const FusedConfig* cfg_inv = nullptr;
+    TransformConfig effective{};
+    int tuned = 0;
+};
+
+namespace nttb {
+
+ntt_status_t validate_modulus(int logN, ModulusConfig m, ModulusRuntime* rt) {
+    const uint64_t N = uint64_t{1} << logN;
+    // same order as make_modulus_runtime (v04:685-707): congruence, then root
+    if (m.qi < 2 || ((uint64_t)m.qi - 1) % (2 * N) != 0)
+        return fail(NTT_ERR_MODULUS, "qi must satisfy qi == 1 mod 2N for negacyclic NTT (q=%u, logN=%d)",
+                    m.qi, logN);
+    if (m.qi >= (1u << 31))
+        return fail(NTT_ERR_MODULUS_RANGE, "modulus %u must be below 2^31", m.qi);
+    if (!hm::is_prime(m.qi)) return fail(NTT_ERR_MODULUS_RANGE, "modulus %u is not prime", m.qi);
+    const uint32_t q = m.qi;
+    const uint32_t psi = hm::powmod(m.primitive_root, ((uint64_t)q - 1) / (2 * N), q);
+    if (hm::powmod(psi, 2 * N, q) != 1 || hm::powmod(psi, N, q) != q - 1)
+        return fail(NTT_ERR_ROOT,
+                    "primitive_root %u did not generate a primitive 2N-th root mod %u",
+                    m.primitive_root, q);
+    if (rt) {
+        rt->qi = q;
+        rt->primitive_root = m.primitive_root;
+        rt->q_inv = hm::neg_qinv(q);
+        rt->r2 = hm::r2_mod(q);
+        rt->psi = psi;
+        rt->psi_inv = hm::powmod(psi, q - 2, q);
+        rt->omega = hm::mulmod(psi, psi, q);
+        rt->degree_inv = hm::powmod((uint32_t)N, q - 2, q);
+    }
+    return NTT_OK;
+}
+
+ntt_status_t check_transform(int logN, const TransformConfig* t) {
+    if (!t) return NTT_OK;
+    const PhaseConfig* ph[4] = {&t->ntt_phase1, &t->ntt_phase2, &t->intt_phase1, &t->intt_phase2};
+    for (auto p : ph)
+        if (p->radix_stages < 0 || p->stage_merging < 0 || p->stage_merging > 5 ||
+            p->warp_batching < 0 || p->warp_batching > 10)
+            return fail(NTT_ERR_INVALID_ARGUMENT, "phase triple out of range");
+    if (t->ntt_phase1.radix_stages + t->ntt_phase2.radix_stages != logN ||
+        t->intt_phase1.radix_stages + t->intt_phase2.radix_stages != logN)
+        return fail(NTT_ERR_INVALID_ARGUMENT,
+                    "phase radix_stages must add up to logN (%d)", logN);
+    return NTT_OK;
+}
+
+// Configuration choice: an explicit phase split selects the compiled
+// configuration with that split, else the tuned entry, else the default.
+void choose_configs(ntt_plan* p, const TransformConfig* t) {
+    p->cfg_fwd = p->cfg_inv = nullptr;
+    if (p->logN <= kSmallMaxLogN || !default_config(p->logN)) return;
+    const FusedConfig* tuned = tuned_config(p->logN, p->limbs);
+    const FusedConfig* def = tuned ? tuned : default_config(p->logN);
+    p->tuned = tuned != nullptr;
+    p->cfg_fwd = p->cfg_inv = def;
+    if (t) {
+        if (auto c = config_by_r1(p->logN, t->ntt_phase1.radix_stages)) p->cfg_fwd = c;
+        if (auto c = config_by_r1(p->logN, t->intt_phase2.radix_stages)) p->cfg_inv = c;
+    }
+}
+
+}  // namespace nttb
+
+extern "C" {
+
+int ntt_version(void) { return NTT_B200_VERSION; }
+
+const char* ntt_status_string(ntt_status_t s) {
+    switch (s) {
+        case NTT_OK: return "ok";
+        case NTT_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case NTT_ERR_MODULUS: return "modulus is not 1 mod 2N";
+        case NTT_ERR_ROOT: return "primitive root does not give a primitive 2N-th root";
+        case NTT_ERR_MODULUS_RANGE: return "modulus must be an odd prime below 2^31";
+        case NTT_ERR_UNSUPPORTED: return "unsupported size";
+        case NTT_ERR_MISALIGNED: return "device pointer not 16-byte aligned";
+        case NTT_ERR_CUDA: return "CUDA error";
+        case NTT_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case NTT_ERR_BUDGET: return "request exceeds the memory budget";
+        case NTT_ERR_TIMEOUT: return "timed out";
+        case NTT_ERR_CANCELLED: return "cancelled";
+        case NTT_ERR_NOT_READY: return "not ready";
+        case NTT_ERR_SHUTDOWN: return "shut down";
+    }
+    return "unknown status";
+}
+
+const char* ntt_last_error(void) { return t_err.c_str(); }
+
+ntt_status_t ntt_modulus_runtime(int logN, ModulusConfig cfg, ModulusRuntime* out) {
+    if (!out) return fail(NTT_ERR_INVALID_ARGUMENT, "out is NULL");
+    if (logN < NTT_MIN_LOGN || logN > 30) return fail(NTT_ERR_UNSUPPORTED, "logN %d", logN);
+    return validate_modulus(logN, cfg, out);
+}
+
+ntt_status_t ntt_twiddle_table_host(int logN, uint32_t q, uint32_t root, uint32_t* out) {
+    if (!out || q < 2) return fail(NTT_ERR_INVALID_ARGUMENT, "bad arguments");
+    if (logN < NTT_MIN_LOGN || logN > 24) return fail(NTT_ERR_UNSUPPORTED, "logN %d", logN);
+    const uint32_t N = 1u << logN;
+    for (uint32_t i = 0; i < N; ++i) out[i] = hm::powmod(root, hm::bitrev(i, logN), q);
+    return NTT_OK;
+}
+
+int ntt_default_moduli(ModulusConfig* out, int cap) {
+    // The reference's default_moduli() list (src/ntt_config.h:75-94).
+    static const ModulusConfig k[16] = {
+        {974258177u, 3u},  {1081212929u, 6u}, {1196556289u, 7u},  {993263617u, 5u},
+        {989986817u, 3u},  {1074266113u, 5u}, {1168900097u, 5u},  {1010565121u, 7u},
+        {957349889u, 6u},  {1073872897u, 7u}, {1209139201u, 31u}, {994705409u, 3u},
+        {998244353u, 3u},  {1073479681u, 11u}, {1158676481u, 3u}, {1016463361u, 38u}};
+    for (int i = 0; out && i < cap && i < 16; ++i) out[i] = k[i];
+    return 16;
+}
+
+ntt_status_t ntt_default_transform(int logN, TransformConfig* out) {
+    // DefaultNTTLaunchConfig<LogN> (src/ntt_config.h:62-73).
+    if (!out) return fail(NTT_ERR_INVALID_ARGUMENT, "out is NULL");
+    if (logN < 10) return fail(NTT_ERR_UNSUPPORTED, "default launch config requires logN >= 10");
+    PhaseConfig a{logN == 16 ? 7 : logN - 9, logN == 16 ? 4 : 3, 4};
+    PhaseConfig b{9, 3, 0};
+    *out = TransformConfig{a, b, b, a};
+    return NTT_OK;
+}
+
+ntt_status_t ntt_find_moduli(int logN, int count, uint32_t lower_bound, ModulusConfig* out) {
+    if (!out || count < 0) return fail(NTT_ERR_INVALID_ARGUMENT, "bad arguments");
+    if (logN < NTT_MIN_LOGN || logN > 29) return fail(NTT_ERR_UNSUPPORTED, "logN %d", logN);
+    const uint64_t step = uint64_t{2} << logN;
+    uint64_t q = lower_bound + ((1 + step - (lower_bound % step)) % step);
+    int found = 0;
+    while (found < count) {
+        if (q >= (uint64_t{1} << 31))
+            return fail(NTT_ERR_MODULUS_RANGE, "ran out of primes below 2^31 (found %d)", found);
+        if (hm::is_prime((uint32_t)q)) {
+            out[found].qi = (uint32_t)q;
+            out[found].primitive_root = hm::smallest_generator((uint32_t)q);
+            ++found;
+        }
+        q += step;
+    }
+    return NTT_OK;
+}
+
+ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int limbs,
+                             const TransformConfig* transform, ntt_plan_t** out) {
+    if (!out) return fail(NTT_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (logN < NTT_MIN_LOGN || logN > NTT_MAX_LOGN)
+        return fail(NTT_ERR_UNSUPPORTED, "logN %d outside [%d, %d]", logN, NTT_MIN_LOGN,
+                    NTT_MAX_LOGN);
+    if (limbs < 1 || !moduli) return fail(NTT_ERR_INVALID_ARGUMENT, "need at least one modulus limb");
+    if (ntt_status_t st = check_transform(logN, transform)) return st;
+    std::vector<TwGenLimb> gf(limbs), gi(limbs);
+    std::vector<uint32_t> qh(limbs);
+    const uint32_t N = 1u << logN;
+    for (int l = 0; l < limbs; ++l) {
+        ModulusRuntime rt;
+        if (ntt_status_t st = validate_modulus(logN, moduli[l], &rt)) return st;
+        const uint32_t q = rt.qi, R = hm::r_mod(q);
+        const uint32_t Rinv = hm::powmod(R, q - 2, q);
+        const uint32_t c = hm::mulmod(rt.degree_inv, Rinv, q);
+        const uint32_t w1 = hm::powmod(rt.psi, hm::bitrev(1, logN), q);
+        const uint32_t w1i = hm::powmod(rt.psi_inv, hm::bitrev(1, logN), q);
+        gf[l] = TwGenLimb{q, rt.q_inv, R, rt.r2, rt.psi, R, hm::mulmod(w1, R, q)};
+        gi[l] = TwGenLimb{q, rt.q_inv, R, rt.r2, rt.psi_inv, c, hm::mulmod(w1i, c, q)};
+        qh[l] = q;
+    }
+    auto* p = new ntt_plan();
+    p->logN = logN;
+    p->limbs = limbs;
+    p->moduli.assign(moduli, moduli + limbs);
+    cudaError_t e = cudaGetDevice(&p->device);
+    const size_t tw_bytes = (size_t)limbs * N * sizeof(TwPair);
+    const size_t q_bytes = ((size_t)limbs * 4 + 255) & ~(size_t)255;
+    p->bytes = 2 * tw_bytes + q_bytes;
+    if (e == cudaSuccess) e = cudaMalloc(&p->block, p->bytes);
+    TwGenLimb* gdev = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&gdev, 2 * limbs * sizeof(TwGenLimb));
+    if (e == cudaSuccess) {
+        p->fwd = (TwPair*)p->block;
+        p->inv = (TwPair*)((char*)p->block + tw_bytes);
+        p->q = (uint32_t*)((char*)p->block + 2 * tw_bytes);
+        e = cudaMemcpy(p->q, qh.data(), limbs * 4, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(gdev, gf.data(), limbs * sizeof(TwGenLimb), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(gdev + limbs, gi.data(), limbs * sizeof(TwGenLimb), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_twiddle_gen(p->fwd, gdev, limbs, logN, 0);
+    if (e == cudaSuccess) e = launch_twiddle_gen(p->inv, gdev + limbs, limbs, logN, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (gdev) cudaFree(gdev);
+    if (e != cudaSuccess) {
+        if (p->block) cudaFree(p->block);
+        delete p;
+        return cuda_fail(e, "plan twiddle generation");
+    }
+    choose_configs(p, transform);
+    effective_triples(p->cfg_fwd, logN, &p->effective);
+    if (p->cfg_inv != p->cfg_fwd) {
+        TransformConfig ti;
+        effective_triples(p->cfg_inv, logN, &ti);
+        p->effective.intt_phase1 = ti.intt_phase1;
+        p->effective.intt_phase2 = ti.intt_phase2;
+    }
+    *out = p;
+    return NTT_OK;
+}
+
+ntt_status_t ntt_plan_destroy(ntt_plan_t* p) {
+    if (!p) return NTT_OK;
+    if (p->block) {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        if (cur != p->device) cudaSetDevice(p->device);
+        cudaFree(p->block);
+        if (cur != p->device) cudaSetDevice(cur);
+    }
+    delete p;
+    return NTT_OK;
+}
+
+ntt_status_t ntt_plan_get_info(const ntt_plan_t* p, ntt_plan_info_t* out) {
+    if (!p || !out) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::memset(out, 0, sizeof *out);
+    out->logN = p->logN;
+    out->limbs = p->limbs;
+    const FusedConfig* c = p->cfg_fwd;
+    out->cluster_ctas = c ? (1 << c->clog) : 1;
+    out->threads_per_cta = c ? c->threads : ((1 << (p->logN - 1)) < 32 ? 32 : (1 << (p->logN - 1)));
+    out->smem_bytes = c ? c->smem_bytes : (4u << p->logN);
+    out->effective = p->effective;
+    out->device_bytes = p->bytes;
+    out->tuned = p->tuned;
+    return NTT_OK;
+}
+
+ntt_status_t ntt_plan_force_config(ntt_plan_t* p, int fwd_index, int inv_index) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    const FusedConfig* f = fwd_index < 0 ? p->cfg_fwd : config_by_index(fwd_index);
+    const FusedConfig* i = inv_index < 0 ? p->cfg_inv : config_by_index(inv_index);
+    if ((fwd_index >= 0 && (!f || f->logN != p->logN)) ||
+        (inv_index >= 0 && (!i || i->logN != p->logN)))
+        return fail(NTT_ERR_INVALID_ARGUMENT, "configuration index does not match logN %d", p->logN);
+    p->cfg_fwd = f;
+    p->cfg_inv = i;
+    effective_triples(p->cfg_fwd, p->logN, &p->effective);
+    TransformConfig ti;
+    effective_triples(p->cfg_inv, p->logN, &ti);
+    p->effective.intt_phase1 = ti.intt_phase1;
+    p->effective.intt_phase2 = ti.intt_phase2;
+    return NTT_OK;
+}
+
+ntt_status_t ntt_plan_tables(const ntt_plan_t* p, const uint32_t** fwd, const uint32_t** inv,
+                             const uint32_t** q) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    if (fwd) *fwd = (const uint32_t*)p->fwd;
+    if (inv) *inv = (const uint32_t*)p->inv;
+    if (q) *q = p->q;
+    return NTT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// transforms
+// ---------------------------------------------------------------------------
+namespace nttb {
+
+ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
+                           int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
+                           cudaStream_t s) {
+    if (polys == 0) return NTT_OK;
+    if (!a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL data pointer");
+    if (((uintptr_t)a & 15u) != 0 || (stride & 3u) != 0)
+        return fail(NTT_ERR_MISALIGNED, "data must be 16-byte aligned (stride a multiple of 4 words)");
+    const size_t N = size_t{1} << logN;
+    if (stride < (size_t)limbs * N && polys > 1)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "poly_stride smaller than limbs * N");
+    const size_t jobs = polys * (size_t)limbs;
+    if (jobs > (size_t)UINT_MAX) return fail(NTT_ERR_INVALID_ARGUMENT, "too many limbs");
+    if (cfg) {
+        FusedArgs fa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride};
+        return launch_fused(cfg, fwd, fa, s);
+    }
+    SmallArgs sa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride, logN};
+    NTT_CUDA_TRY(launch_small(sa, fwd, s), "small NTT launch");
+    return NTT_OK;
+}
+
+static ntt_status_t plan_run(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
+                             bool fwd, ntt_stream_t s) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    int dev = 0;
+    NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev != p->device)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "plan was created on device %d, current is %d",
+                    p->device, dev);
+    if (stride == 0) stride = (size_t)p->limbs << p->logN;
+    return run_transform(p->logN, fwd ? p->cfg_fwd : p->cfg_inv, fwd ? p->fwd : p->inv, p->q,
+                         p->limbs, a, polys, stride, fwd, (cudaStream_t)s);
+}
+
+}  // namespace nttb
+
+extern "C" {
+
+ntt_status_t ntt_forward(const ntt_plan_t* p, uint32_t* a, ntt_stream_t s) {
+    return plan_run(p, a, 1, 0, true, s);
+}
+ntt_status_t ntt_inverse(const ntt_plan_t* p, uint32_t* a, ntt_stream_t s) {
+    return plan_run(p, a, 1, 0, false, s);
+}
+ntt_status_t ntt_forward_many(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
+                              ntt_stream_t s) {
+    return plan_run(p, a, polys, stride, true, s);
+}
+ntt_status_t ntt_inverse_many(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
+                              ntt_stream_t s) {
+    return plan_run(p, a, polys, stride, false, s);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// drop-in launchers over the reference's Montgomery tables
+// ---------------------------------------------------------------------------
+namespace {
+struct ShimKey {
+    int dev;
+    const void* tw;
+    const void* moduli;
+    const void* qinv;
+    const void* aux;
+    size_t limbs;
+    int logN;
+    int inverse;
+    bool operator<(const ShimKey& o) const {
+        return std::tie(dev, tw, moduli, qinv, aux, limbs, logN, inverse) <
+               std::tie(o.dev, o.tw, o.moduli, o.qinv, o.aux, o.limbs, o.logN, o.inverse);
+    }
+};
+std::mutex g_shim_mu;
+std::map<ShimKey, TwPair*> g_shim;
+
+ntt_status_t shim_run(uint32_t* A, const uint32_t* tw, const uint32_t* moduli, const uint32_t* qinv,
+                      const uint32_t* aux, size_t limbs, int logN, const PhaseConfig* ph1,
+                      const PhaseConfig* ph2, bool inverse) {
+    if (!A || !tw || !moduli || !qinv || !aux)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "NULL device pointer");
+    if (logN < NTT_MIN_LOGN || logN > NTT_MAX_LOGN) return fail(NTT_ERR_UNSUPPORTED, "logN %d", logN);
+    if (limbs == 0) return NTT_OK;
+    if (limbs > (1u << 20)) return fail(NTT_ERR_INVALID_ARGUMENT, "limb_count too large");
+    if (ph1 && ph2 && ph1->radix_stages + ph2->radix_stages != logN)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "phase radix_stages must add up to logN");
+    int dev = 0;
+    NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    ShimKey k{dev, tw, moduli, qinv, aux, limbs, logN, inverse ? 1 : 0};
+    TwPair* table = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_shim_mu);
+        auto it = g_shim.find(k);
+        if (it != g_shim.end()) table = it->second;
+    }
+    if (!table) {
+        const size_t N = size_t{1} << logN;
+        NTT_CUDA_TRY(cudaMalloc(&table, limbs * N * sizeof(TwPair)), "cudaMalloc(shim table)");
+        cudaError_t e = launch_twiddle_import(table, tw, moduli, qinv, aux, (int)limbs, logN,
+                                              inverse ? 1 : 0, 0);
+        if (e != cudaSuccess) {
+            cudaFree(table);
+            return cuda_fail(e, "twiddle import");
+        }
+        std::lock_guard<std::mutex> lk(g_shim_mu);
+        auto ins = g_shim.insert({k, table});
+        if (!ins.second) {  // another thread won the race
+            cudaFree(table);
+            table = ins.first->second;
+        }
+    }
+    const FusedConfig* cfg = nullptr;
+    if (logN > kSmallMaxLogN) {
+        // column stages: NTT phase 1 / INTT phase 2 (the second triple)
+        const PhaseConfig* col = inverse ? ph2 : ph1;
+        cfg = col ? config_by_r1(logN, col->radix_stages) : nullptr;
+        if (!cfg) cfg = tuned_config(logN, (int)limbs);
+        if (!cfg) cfg = default_config(logN);
+    }
+    return run_transform(logN, cfg, table, moduli, (int)limbs, A, 1, limbs << logN, !inverse, 0);
+}
+}  // namespace
+
+extern "C" {
+
+ntt_status_t ntt_launch_ntt(uint32_t* A, const uint32_t* tw, const uint32_t* moduli,
+                            const uint32_t* q_inv, const uint32_t* r2, size_t limb_count, int logN,
+                            const PhaseConfig* phase1, const PhaseConfig* phase2) {
+    return shim_run(A, tw, moduli, q_inv, r2, limb_count, logN, phase1, phase2, false);
+}
+
+ntt_status_t ntt_launch_intt(uint32_t* A, const uint32_t* itw, const uint32_t* moduli,
+                             const uint32_t* q_inv, const uint32_t* degree_inv, size_t limb_count,
+                             int logN, const PhaseConfig* phase1, const PhaseConfig* phase2) {
+    return shim_run(A, itw, moduli, q_inv, degree_inv, limb_count, logN, phase1, phase2, true);
+}
+
+void ntt_shim_cache_clear(void) {
+    std::lock_guard<std::mutex> lk(g_shim_mu);
+    for (auto& kv : g_shim) {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        if (cur != kv.first.dev) cudaSetDevice(kv.first.dev);
+        cudaFree(kv.second);
+        if (cur != kv.first.dev) cudaSetDevice(cur);
+    }
+    g_shim.clear();
+}
+
+}  // extern "C"

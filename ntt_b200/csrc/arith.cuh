@@ -1,0 +1,145 @@
+// Exact 32-bit modular arithmetic for the NTT kernels (host + device).
+//
+// The reference (src/v04_montgomery.cu:93-146) keeps every value canonical in
+// [0, q) and multiplies with 32-bit Montgomery REDC (4 multiplies + 2
+// conditional corrections per product).  On sm_100a the transform is bound by
+// integer issue, so the kernels here use Shoup's precomputed-quotient product
+// (3 multiplies) with Harvey's lazy reduction ranges instead:
+//
+//   shoup(a, w, w') = a*w - umulhi(a, w')*q   (mod 2^32),  w' = floor(w*2^32/q)
+//   -> a*w mod q  + {0, q}  for any a < 2^32, 0 <= w < q < 2^31.
+//
+// Two range disciplines ("kinds"), chosen per limb from its modulus:
+//   Lazy4 (q < 2^30): CT butterflies keep values in [0, 4q), GS in [0, 2q);
+//                     7 integer instructions per butterfly.
+//   Lazy2 (q < 2^31): CT in [0, 2q), GS in [0, q); 9 instructions.
+// Every transform ends with a canonicalisation to [0, q), so outputs are the
+// unique residues and therefore bit-identical to the reference's.
+#pragma once
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define NTT_HD __host__ __device__ __forceinline__
+#else
+#define NTT_HD inline
+#endif
+
+namespace nttb {
+
+NTT_HD uint32_t mulhi32(uint32_t a, uint32_t b) {
+#if defined(__CUDA_ARCH__)
+    return __umulhi(a, b);
+#else
+    return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
+NTT_HD uint32_t umin32(uint32_t a, uint32_t b) {
+#if defined(__CUDA_ARCH__)
+    return min(a, b);
+#else
+    return a < b ? a : b;
+#endif
+}
+
+// x in [0, 2m) -> [0, m).  Unsigned wrap makes x - m huge when x < m.
+NTT_HD uint32_t csub(uint32_t x, uint32_t m) { return umin32(x, x - m); }
+
+// Shoup product: result congruent to a*w (mod q), in [0, 2q).
+NTT_HD uint32_t shoup_mul(uint32_t a, uint32_t w, uint32_t wp, uint32_t q) {
+    uint32_t h = mulhi32(a, wp);
+    return a * w - h * q;
+}
+
+// A twiddle as stored on the device: value and Shoup companion.
+struct TwPair {
+    uint32_t w;
+    uint32_t wp;
+};
+
+// ---- butterflies ----------------------------------------------------------
+
+struct Lazy4 {  // q < 2^30
+    static constexpr bool kLazy4 = true;
+    // Cooley-Tukey: (X, Y) -> (X + wY, X - wY); in/out ranges [0, 4q).
+    NTT_HD static void ct(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q,
+                          uint32_t q2) {
+        uint32_t a = csub(x, q2);
+        uint32_t t = shoup_mul(y, w, wp, q);
+        x = a + t;
+        y = a - t + q2;
+    }
+    // First forward stage with the normal->Montgomery factor R folded in:
+    // (X, Y) -> (R X + (wR) Y, R X - (wR) Y); any 32-bit input.
+    NTT_HD static void ct_first(uint32_t& x, uint32_t& y, TwPair r, TwPair wr, uint32_t q,
+                                uint32_t q2) {
+        uint32_t a = shoup_mul(x, r.w, r.wp, q);
+        uint32_t t = shoup_mul(y, wr.w, wr.wp, q);
+        x = a + t;
+        y = a - t + q2;
+    }
+    // Forward output range [0, 4q) -> canonical.
+    NTT_HD static uint32_t fwd_final(uint32_t v, uint32_t q, uint32_t q2) {
+        return csub(csub(v, q2), q);
+    }
+    // Gentleman-Sande: (X, Y) -> (X + Y, (X - Y) w); in/out ranges [0, 2q).
+    NTT_HD static void gs(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q,
+                          uint32_t q2) {
+        uint32_t s = x + y;
+        uint32_t d = x - y + q2;
+        x = csub(s, q2);
+        y = shoup_mul(d, w, wp, q);
+    }
+    // Last inverse stage with c = N^{-1} R^{-1} folded in, canonical output:
+    // (X, Y) -> ((X + Y) c, (X - Y) (w c)).
+    NTT_HD static void gs_last(uint32_t& x, uint32_t& y, TwPair c, TwPair wc, uint32_t q,
+                               uint32_t q2) {
+        uint32_t s = x + y;
+        uint32_t d = x - y + q2;
+        x = csub(shoup_mul(s, c.w, c.wp, q), q);
+        y = csub(shoup_mul(d, wc.w, wc.wp, q), q);
+    }
+};
+
+struct Lazy2 {  // q < 2^31
+    static constexpr bool kLazy4 = false;
+    // ranges [0, 2q)
+    NTT_HD static void ct(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q,
+                          uint32_t) {
+        uint32_t a = csub(x, q);
+        uint32_t t = csub(shoup_mul(y, w, wp, q), q);
+        x = a + t;
+        y = a - t + q;
+    }
+    NTT_HD static void ct_first(uint32_t& x, uint32_t& y, TwPair r, TwPair wr, uint32_t q,
+                                uint32_t) {
+        uint32_t a = csub(shoup_mul(x, r.w, r.wp, q), q);
+        uint32_t t = csub(shoup_mul(y, wr.w, wr.wp, q), q);
+        x = a + t;
+        y = a - t + q;
+    }
+    NTT_HD static uint32_t fwd_final(uint32_t v, uint32_t q, uint32_t) { return csub(v, q); }
+    // ranges [0, q)
+    NTT_HD static void gs(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q,
+                          uint32_t) {
+        uint32_t s = x + y;
+        uint32_t d = x - y + q;
+        x = csub(s, q);
+        y = csub(shoup_mul(d, w, wp, q), q);
+    }
+    NTT_HD static void gs_last(uint32_t& x, uint32_t& y, TwPair c, TwPair wc, uint32_t q,
+                               uint32_t) {
+        uint32_t s = x + y;
+        uint32_t d = x - y + q;
+        x = csub(shoup_mul(s, c.w, c.wp, q), q);
+        y = csub(shoup_mul(d, wc.w, wc.wp, q), q);
+    }
+};
+
+// ---- host-side helpers for table construction ------------------------------
+
+inline uint32_t shoup_companion(uint32_t w, uint32_t q) {
+    return (uint32_t)(((uint64_t)w << 32) / q);
+}
+
+}  // namespace nttb

@@ -1,0 +1,46 @@
+// Compiled fused-kernel configurations.
+//
+// X(LOGN, CLOG, R1, EB, K1A, K2A):
+//   LOGN  log2 N of the limb
+//   CLOG  log2 of the thread-block cluster size (CTAs per limb)
+//   R1    stages of phase 1 (the reference's NTT-Phase1 radix_stages); phase 2
+//         does LOGN - R1 (its NTT-Phase2 radix_stages)
+//   EB    log2 words per thread in a register pass (the reference's
+//         stage_merging upper bound: a pass merges up to EB radix-2 stages)
+//   K1A   stages of the first register pass of phase 1 (rest: second pass)
+//   K2A   stages of the first register pass of phase 2
+// Each logN has its own list so the instantiations compile in parallel.
+#pragma once
+
+#define NTTB_CFG_N10(X) X(10, 0, 5, 5, 5, 5)
+#define NTTB_CFG_N11(X) X(11, 0, 6, 5, 1, 5)
+#define NTTB_CFG_N12(X) X(12, 0, 7, 5, 3, 5)
+#define NTTB_CFG_N13(X) X(13, 0, 8, 5, 3, 5)
+#define NTTB_CFG_N14(X) X(14, 0, 9, 5, 4, 5) X(14, 1, 9, 5, 4, 5)
+#define NTTB_CFG_N15(X) X(15, 1, 10, 5, 5, 5) X(15, 2, 8, 5, 3, 4)
+#define NTTB_CFG_N16(X) \
+    X(16, 3, 8, 5, 3, 4) X(16, 3, 7, 5, 3, 5) X(16, 2, 8, 5, 3, 4) X(16, 4, 8, 5, 3, 4) \
+    X(16, 3, 8, 4, 4, 4)
+#define NTTB_CFG_N17(X) X(17, 3, 8, 5, 3, 5) X(17, 4, 8, 5, 3, 5)
+
+#define NTTB_CFG_ALL(X)                                                                      \
+    NTTB_CFG_N10(X) NTTB_CFG_N11(X) NTTB_CFG_N12(X) NTTB_CFG_N13(X) NTTB_CFG_N14(X)      \
+    NTTB_CFG_N15(X) NTTB_CFG_N16(X) NTTB_CFG_N17(X)
+
+#include <cstdint>
+
+namespace nttb {
+
+struct FusedConfig {
+    int logN, clog, r1, eb, k1a, k2a;
+    int threads;
+    uint32_t smem_bytes;
+    const void* fwd;  // __global__ fused_kernel<G, true>
+    const void* inv;  // __global__ fused_kernel<G, false>
+};
+
+// All compiled configurations (registry.cu); count via fused_config_count().
+const FusedConfig* fused_configs();
+int fused_config_count();
+
+}  // namespace nttb

@@ -1,0 +1,13 @@
+// Instantiations of the fused kernel for logN = 17 (see configs.h).
+#include "../configs.h"
+#include "../fused_kernel.cuh"
+
+namespace nttb {
+#define NTTB_ENTRY(N, CL, R1, EB, K1A, K2A)                                                  \
+    {N, CL, R1, EB, K1A, K2A, Geometry<N, CL, R1, EB, K1A, K2A>::THREADS,                   \
+     Geometry<N, CL, R1, EB, K1A, K2A>::SMEM_BYTES,                                         \
+     (const void*)&fused_kernel<Geometry<N, CL, R1, EB, K1A, K2A>, true>,                   \
+     (const void*)&fused_kernel<Geometry<N, CL, R1, EB, K1A, K2A>, false>},
+extern const FusedConfig kFusedN17[] = {NTTB_CFG_N17(NTTB_ENTRY)};
+extern const int kFusedN17Count = sizeof(kFusedN17) / sizeof(kFusedN17[0]);
+}  // namespace nttb

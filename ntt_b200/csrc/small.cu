@@ -1,0 +1,67 @@
+// Transforms of small limbs (N <= 2^9): one CTA per limb, one shared-memory
+// round per radix-2 stage.  Same table layout, folds and lazy arithmetic as
+// the fused kernels; these sizes are latency-bound, not throughput-bound.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "arith.cuh"
+#include "small.h"
+
+namespace nttb {
+
+template <class Arith, bool Fwd>
+__device__ void small_body(uint32_t* a, const TwPair* tw, uint32_t q, int logN, uint32_t* s) {
+    const uint32_t N = 1u << logN, half = N >> 1, q2 = 2u * q;
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) s[i] = a[i];
+    __syncthreads();
+    for (int st = 0; st < logN; ++st) {
+        // forward: stage st (t = N >> (st+1)); inverse: stage logN-1-st
+        const int sg = Fwd ? st : (logN - 1 - st);
+        const uint32_t t = N >> (sg + 1);
+        for (uint32_t b = threadIdx.x; b < half; b += blockDim.x) {
+            const uint32_t j = b / t, k = j * 2 * t + (b % t);
+            uint32_t x = s[k], y = s[k + t];
+            if (Fwd) {
+                if (sg == 0) Arith::ct_first(x, y, tw[0], tw[1], q, q2);
+                else {
+                    const TwPair w = tw[(1u << sg) + j];
+                    Arith::ct(x, y, w.w, w.wp, q, q2);
+                }
+            } else {
+                if (sg == 0) Arith::gs_last(x, y, tw[0], tw[1], q, q2);
+                else {
+                    const TwPair w = tw[(1u << sg) + j];
+                    Arith::gs(x, y, w.w, w.wp, q, q2);
+                }
+            }
+            s[k] = x;
+            s[k + t] = y;
+        }
+        __syncthreads();
+    }
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x)
+        a[i] = Fwd ? Arith::fwd_final(s[i], q, q2) : s[i];
+}
+
+template <bool Fwd>
+__global__ void small_kernel(SmallArgs p) {
+    __shared__ uint32_t s[1u << kSmallMaxLogN];
+    const uint32_t job = blockIdx.x;
+    const uint32_t limb = job % p.limbs, poly = job / p.limbs;
+    uint32_t* a = p.data + (size_t)poly * p.poly_stride + ((size_t)limb << p.logN);
+    const TwPair* tw = p.tw + ((size_t)limb << p.logN);
+    const uint32_t q = p.q[limb];
+    if (q < (1u << 30)) small_body<Lazy4, Fwd>(a, tw, q, p.logN, s);
+    else small_body<Lazy2, Fwd>(a, tw, q, p.logN, s);
+}
+
+cudaError_t launch_small(const SmallArgs& a, bool fwd, cudaStream_t s) {
+    if (a.logN < 1 || a.logN > kSmallMaxLogN) return cudaErrorInvalidValue;
+    if (a.jobs == 0) return cudaSuccess;
+    const uint32_t half = 1u << (a.logN - 1);
+    dim3 block(half < 32 ? 32 : half), grid(a.jobs);
+    if (fwd) small_kernel<true><<<grid, block, 0, s>>>(a);
+    else small_kernel<false><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace nttb

@@ -1,0 +1,18 @@
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "arith.cuh"
+
+namespace nttb {
+constexpr int kSmallMaxLogN = 9;
+struct SmallArgs {
+    uint32_t* data;
+    const TwPair* tw;
+    const uint32_t* q;
+    uint32_t limbs;
+    uint32_t jobs;
+    unsigned long long poly_stride;
+    int logN;
+};
+cudaError_t launch_small(const SmallArgs& a, bool fwd, cudaStream_t s);
+}  // namespace nttb

@@ -1,0 +1,103 @@
+// Device-side twiddle generation and import (sm_100a).
+//
+// Table layout (per limb, N entries of (w, w') uint32 pairs, w' the Shoup
+// companion floor(w * 2^32 / q)):
+//   forward  entry i >= 2: psi^bitrev(i)      (the reference's
+//            make_twiddle_table, src/v04_montgomery.cu:720-727, kept in the
+//            normal domain because Shoup products need no Montgomery form)
+//            entry 0: R mod q            (R = 2^32; folded normal->Montgomery
+//                                         conversion of the input, v04:229-232)
+//            entry 1: psi^bitrev(1) * R  (limb stage 0's only twiddle, with R)
+//   inverse  entry i >= 2: psi^-bitrev(i)
+//            entry 0: c = N^-1 * R^-1    (the reference's NormalizeKernel,
+//                                         v04:567-580, folded into the last
+//                                         stage: N^-1 and from_mont)
+//            entry 1: psi^-bitrev(1) * c
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "arith.cuh"
+#include "twiddle.h"
+
+namespace nttb {
+
+__device__ __forceinline__ uint32_t dev_redc(uint64_t t, uint32_t q, uint32_t nqinv) {
+    uint32_t m = (uint32_t)t * nqinv;
+    uint64_t u = (t + (uint64_t)m * q) >> 32;
+    return (uint32_t)(u >= q ? u - q : u);
+}
+
+__device__ __forceinline__ uint32_t dev_brev(uint32_t v, int width) {
+    return __brev(v) >> (32 - width);
+}
+
+// One thread per table entry; blockIdx.y = limb.
+__global__ void twiddle_gen_kernel(TwPair* out, const TwGenLimb* limbs, int logN) {
+    const uint32_t N = 1u << logN;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const TwGenLimb L = limbs[blockIdx.y];
+    uint32_t w;
+    if (i == 0) {
+        w = L.fold0;
+    } else if (i == 1) {
+        w = L.fold1;
+    } else {
+        // base^bitrev(i) by Montgomery square-and-multiply (q < 2^31)
+        uint32_t e = dev_brev(i, logN);
+        uint32_t x = dev_redc((uint64_t)L.base * L.r2, L.q, L.nqinv);  // base * R
+        uint32_t acc = L.r_mod;                                          // 1 * R
+        while (e) {
+            if (e & 1u) acc = dev_redc((uint64_t)acc * x, L.q, L.nqinv);
+            x = dev_redc((uint64_t)x * x, L.q, L.nqinv);
+            e >>= 1;
+        }
+        w = dev_redc(acc, L.q, L.nqinv);  // leave the Montgomery domain
+    }
+    out[(size_t)blockIdx.y * N + i] = TwPair{w, (uint32_t)(((uint64_t)w << 32) / L.q)};
+}
+
+// Import the reference's Montgomery-form tables (tw_mont[i] = to_mont(w_i)).
+// Forward: fold0 = R = redc(r2), fold1 = tw_mont[1] itself (= w_1 * R).
+// Inverse: fold0 = c = redc(redc(degree_inv_mont)), fold1 = w_1 * c.
+__global__ void twiddle_import_kernel(TwPair* out, const uint32_t* tw_mont,
+                                      const uint32_t* moduli, const uint32_t* nqinv,
+                                      const uint32_t* aux, int logN, int inverse) {
+    const uint32_t N = 1u << logN;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const uint32_t l = blockIdx.y;
+    const uint32_t q = moduli[l], qi = nqinv[l];
+    const uint32_t* t = tw_mont + (size_t)l * N;
+    uint32_t w;
+    if (!inverse) {
+        if (i == 0) w = dev_redc(aux[l], q, qi);
+        else if (i == 1) w = t[1] % q;
+        else w = dev_redc(t[i], q, qi);
+    } else {
+        const uint32_t c = dev_redc(dev_redc(aux[l], q, qi), q, qi);
+        if (i == 0) w = c;
+        else if (i == 1) w = (uint32_t)(((uint64_t)dev_redc(t[1], q, qi) * c) % q);
+        else w = dev_redc(t[i], q, qi);
+    }
+    out[(size_t)l * N + i] = TwPair{w, (uint32_t)(((uint64_t)w << 32) / q)};
+}
+
+cudaError_t launch_twiddle_gen(TwPair* out, const TwGenLimb* limbs_dev, int limbs, int logN,
+                               cudaStream_t s) {
+    const uint32_t N = 1u << logN;
+    dim3 block(N < 256 ? N : 256), grid((N + block.x - 1) / block.x, limbs);
+    twiddle_gen_kernel<<<grid, block, 0, s>>>(out, limbs_dev, logN);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_twiddle_import(TwPair* out, const uint32_t* tw_mont, const uint32_t* moduli,
+                                  const uint32_t* nqinv, const uint32_t* aux, int limbs,
+                                  int logN, int inverse, cudaStream_t s) {
+    const uint32_t N = 1u << logN;
+    dim3 block(N < 256 ? N : 256), grid((N + block.x - 1) / block.x, limbs);
+    twiddle_import_kernel<<<grid, block, 0, s>>>(out, tw_mont, moduli, nqinv, aux, logN,
+                                                 inverse);
+    return cudaGetLastError();
+}
+
+}  // namespace nttb

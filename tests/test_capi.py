@@ -1,0 +1,124 @@
+"""The C ABI without a GPU: the library loads, exports every declared entry
+point, and its host-side precompute matches the oracle and the reference's
+error behaviour (status codes where the reference exits)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import ntt_b200 as nb
+from oracle import oracle as O
+
+INCLUDE = os.path.join(os.path.dirname(__file__), "..", "include")
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(INCLUDE):
+        if fn.endswith(".h"):
+            src = open(os.path.join(INCLUDE, fn)).read()
+            names |= set(re.findall(r"^NTT_API [^(]*?\b(ntt_\w+)\(", src, re.M))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_exported():
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(nb._lib, s), s
+
+
+def test_version_and_status_strings():
+    assert nb.version() == 100
+    for code in nb.STATUS_NAMES:
+        assert nb._lib.ntt_status_string(code)
+
+
+def test_default_moduli_is_reference_list():
+    assert [tuple(m) for m in nb.default_moduli()] == O.REFERENCE_DEFAULT_MODULI
+
+
+def test_default_transform_matches_default_launch_config():
+    t = nb.default_transform(16)
+    assert t.ntt_phase1.as_tuple() == (7, 4, 4) and t.intt_phase2.as_tuple() == (7, 4, 4)
+    assert t.ntt_phase2.as_tuple() == (9, 3, 0) and t.intt_phase1.as_tuple() == (9, 3, 0)
+    t = nb.default_transform(12)
+    assert t.ntt_phase1.as_tuple() == (3, 3, 4)
+    with pytest.raises(nb.NttError) as e:
+        nb.default_transform(9)  # static_assert(LogN >= 10) in the reference
+    assert e.value.name == "NTT_ERR_UNSUPPORTED"
+
+
+@pytest.mark.parametrize("logN", [1, 10, 16, 17])
+def test_modulus_runtime_matches_oracle(logN):
+    for q, g in O.REFERENCE_DEFAULT_MODULI[:6] if logN <= 16 else O.ascending_primes(17, 4, 1 << 30):
+        rt = nb.modulus_runtime(logN, (q, g))
+        st, ort = O.modulus_runtime(logN, q, g)
+        assert st == 0
+        assert tuple(getattr(rt, n) for n, _ in rt._fields_) == ort.as_tuple()
+
+
+def test_modulus_errors_mirror_reference_exits():
+    with pytest.raises(nb.NttError) as e:
+        nb.modulus_runtime(16, (974258177 + 2, 3))
+    assert e.value.name == "NTT_ERR_MODULUS"
+    with pytest.raises(nb.NttError) as e:
+        nb.modulus_runtime(16, (974258177, 1))
+    assert e.value.name == "NTT_ERR_ROOT"
+    with pytest.raises(nb.NttError) as e:  # even q: fails the congruence, as in v04
+        nb.modulus_runtime(4, (64, 3))
+    assert e.value.name == "NTT_ERR_MODULUS"
+    with pytest.raises(nb.NttError) as e:  # composite q == 1 mod 2N
+        nb.modulus_runtime(4, (33 * 32 + 1, 3))
+    assert e.value.name in ("NTT_ERR_MODULUS_RANGE", "NTT_ERR_ROOT")
+    with pytest.raises(nb.NttError) as e:  # 32-bit prime: beyond the 2^31 bound
+        q = next(q for q in range((1 << 31) + 1, (1 << 32), 1 << 17) if O.is_prime_u32(q))
+        nb.modulus_runtime(16, (q, O.smallest_generator(q)))
+    assert e.value.name == "NTT_ERR_MODULUS_RANGE"
+
+
+@pytest.mark.parametrize("logN", [2, 9, 16])
+def test_twiddle_table_matches_oracle(logN):
+    q, g = O.ascending_primes(logN, 1, int(2 ** 30.5))[0]
+    _, rt = O.modulus_runtime(logN, q, g)
+    assert np.array_equal(nb.twiddle_table(logN, q, rt.psi), O.twiddle_table(logN, q, rt.psi))
+
+
+@pytest.mark.parametrize("logN,count,start", [(16, 16, 974258177), (17, 8, int(2 ** 29.5)),
+                                              (12, 64, int(2 ** 30.5))])
+def test_find_moduli_matches_oracle(logN, count, start):
+    got = [tuple(m) for m in nb.find_moduli(logN, count, start)]
+    assert got == O.ascending_primes(logN, count, start)
+
+
+def test_config_catalogue_covers_every_size():
+    cfgs = nb.kernel_configs()
+    assert {c.logN for c in cfgs} == set(range(10, 18))
+    for c in cfgs:
+        assert c.threads in (32, 64, 128, 256, 512, 1024)
+        assert c.smem_bytes <= 227 * 1024
+        assert c.cluster_ctas in (1, 2, 4, 8, 16)
+
+
+def test_plan_without_device_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(nb.NttError) as e:
+        nb.Plan(12, O.ascending_primes(12, 2, 1 << 29))
+    assert e.value.name in ("NTT_ERR_CUDA", "NTT_ERR_OUT_OF_MEMORY")
+
+
+def test_invalid_plan_arguments():
+    with pytest.raises(nb.NttError) as e:
+        nb.Plan(18, [(974258177, 3)])
+    assert e.value.name == "NTT_ERR_UNSUPPORTED"
+    with pytest.raises(nb.NttError) as e:
+        nb.Plan(16, [])
+    assert e.value.name == "NTT_ERR_INVALID_ARGUMENT"
+    bad = nb.default_transform(16)
+    bad.ntt_phase2.radix_stages = 8  # 7 + 8 != 16
+    with pytest.raises(nb.NttError) as e:
+        nb.Plan(16, [(974258177, 3)], bad)
+    assert e.value.name == "NTT_ERR_INVALID_ARGUMENT"

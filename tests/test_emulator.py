@@ -1,0 +1,64 @@
+"""Index maps of every compiled fused-kernel configuration, checked on the CPU.
+
+tests/emu/libntt_emu.so runs the device kernels' pass functions
+(ntt_b200/csrc/ntt_core.cuh) thread by thread on the host.  Each
+configuration must reproduce the oracle bit for bit (forward and inverse,
+30- and 31-bit moduli), never access out of bounds, write every word exactly
+once per step, and keep warp-wide shared-memory bank conflicts bounded.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from twiddle_ref import device_tables
+
+EMU_DIR = os.path.join(os.path.dirname(__file__), "emu")
+
+
+@pytest.fixture(scope="module")
+def emu():
+    subprocess.run(["make", "-s", "-C", EMU_DIR], check=True, capture_output=True)
+    E = ctypes.CDLL(os.path.join(EMU_DIR, "libntt_emu.so"))
+    E.emu_transform.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    E.emu_last_error.restype = ctypes.c_char_p
+    return E
+
+
+def configs():
+    # parsed from the same X-list the library compiles
+    import re
+    src = open(os.path.join(os.path.dirname(__file__), "..", "ntt_b200", "csrc", "configs.h")).read()
+    body = src.split("#define NTTB_CFG_ALL")[0]
+    return [tuple(int(v) for v in m) for m in
+            re.findall(r"X\((\d+), (\d+), (\d+), (\d+), (\d+), (\d+)\)", body)]
+
+
+@pytest.mark.parametrize("idx,cfg", list(enumerate(configs())), ids=lambda v: str(v))
+@pytest.mark.parametrize("bits", [30, 31])
+def test_config_matches_oracle(emu, idx, cfg, bits):
+    c = (ctypes.c_int * 8)()
+    emu.emu_config(idx, c)
+    assert tuple(c)[:6] == cfg
+    logN = cfg[0]
+    start = int(2 ** 29.5) if bits == 30 else int(2 ** 30.5)
+    mods = O.ascending_primes(logN, 2, start)
+    T = O.LimbTables(logN, mods)
+    fwd, inv = device_tables(T)
+    x = O.uniform_limbs(logN, T.q, 100 + idx)
+    x[0, :4] = [0, 1, T.q[0] - 1, 0xFFFFFFFF]  # edge values (forward reduces any uint32)
+    d = x.copy()
+    st = (ctypes.c_double * 2)()
+    rc = emu.emu_transform(idx, 1, d.ctypes.data, fwd.ctypes.data, T.q.ctypes.data, 2, st)
+    assert rc == 0, emu.emu_last_error().decode()
+    assert np.array_equal(d, T.forward_mont(x))
+    assert st[0] <= 16  # worst warp-wide bank conflict degree
+    rc = emu.emu_transform(idx, 0, d.ctypes.data, inv.ctypes.data, T.q.ctypes.data, 2, st)
+    assert rc == 0, emu.emu_last_error().decode()
+    expect = x.copy()
+    expect[0, 3] = 0xFFFFFFFF % T.q[0]
+    assert np.array_equal(d, expect)

@@ -1,0 +1,39 @@
+"""Device twiddle-table layout built from the oracle's tables (test helper).
+
+The product's device tables (ntt_b200/csrc/twiddle.cu) hold, per limb, N
+(w, w') pairs: w = psi^bitrev(i) (forward) or psi^-bitrev(i) (inverse), w' its
+Shoup companion floor(w * 2^32 / q), with entries 0 and 1 replaced by the
+constants folded into limb stage 0:
+  forward  [0] = R mod q, [1] = psi^bitrev(1) * R   (R = 2^32: Montgomery form)
+  inverse  [0] = c = N^-1 * R^-1, [1] = psi^-bitrev(1) * c
+This module rebuilds that layout from the oracle so the CPU emulator and the
+GPU table check have an independent expected value.
+"""
+import numpy as np
+
+
+def _pair(w: int, q: int):
+    return (w % q, ((w % q) << 32) // q)
+
+
+def device_tables(T):
+    """T: oracle.LimbTables -> (fwd_pairs, inv_pairs), each uint32[L, N, 2]."""
+    L, N = T.psi_tab.shape
+    fwd = np.empty((L, N, 2), dtype=np.uint32)
+    inv = np.empty((L, N, 2), dtype=np.uint32)
+    for l, (q, _) in enumerate(T.moduli):
+        qq = np.uint64(q)
+        w = T.psi_tab[l].astype(np.uint64)
+        fwd[l, :, 0] = w
+        fwd[l, :, 1] = ((w << np.uint64(32)) // qq).astype(np.uint32)
+        w = T.inv_tab[l].astype(np.uint64)
+        inv[l, :, 0] = w
+        inv[l, :, 1] = ((w << np.uint64(32)) // qq).astype(np.uint32)
+        R = (1 << 32) % q
+        Rinv = pow(R, q - 2, q)
+        c = int(T.degree_inv[l]) * Rinv % q
+        fwd[l, 0] = _pair(R, q)
+        fwd[l, 1] = _pair(int(T.psi_tab[l, 1]) * R, q)
+        inv[l, 0] = _pair(c, q)
+        inv[l, 1] = _pair(int(T.inv_tab[l, 1]) * c, q)
+    return fwd, inv
