@@ -433,8 +433,11 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
                            cudaStream_t s) {
     if (polys == 0) return NTT_OK;
     if (!a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL data pointer");
-    if (((uintptr_t)a & 15u) != 0 || (stride & 3u) != 0)
+    // the fused kernels move 16-byte vectors; the small-size kernel words
+    if (cfg && (((uintptr_t)a & 15u) != 0 || (polys > 1 && (stride & 3u) != 0)))
         return fail(NTT_ERR_MISALIGNED, "data must be 16-byte aligned (stride a multiple of 4 words)");
+    if (((uintptr_t)a & 3u) != 0)
+        return fail(NTT_ERR_MISALIGNED, "data must be 4-byte aligned");
     const size_t N = size_t{1} << logN;
     if (stride < (size_t)limbs * N && polys > 1)
         return fail(NTT_ERR_INVALID_ARGUMENT, "poly_stride smaller than limbs * N");
