@@ -140,6 +140,10 @@ NTT_API ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int 
                              const TransformConfig* transform, ntt_plan_t** out);
 NTT_API ntt_status_t ntt_plan_destroy(ntt_plan_t* plan);
 NTT_API ntt_status_t ntt_plan_get_info(const ntt_plan_t* plan, ntt_plan_info_t* out);
+/* Waits for the device, then reads and clears the plan's device status word
+ * (bit 0: a bounded wait inside a transform kernel expired -- returned as
+ * NTT_ERR_TIMEOUT).  device_status may be NULL. */
+NTT_API ntt_status_t ntt_plan_check(const ntt_plan_t* plan, uint32_t* device_status);
 /* Device pointers of the plan's tables: limbs * N (w, w') uint32 pairs, with
  * entries 0 and 1 holding the constants folded into limb stage 0. */
 NTT_API ntt_status_t ntt_plan_tables(const ntt_plan_t* plan, const uint32_t** fwd_pairs,

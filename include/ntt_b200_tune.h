@@ -1,5 +1,5 @@
 /*
- * ntt_b200 autotuner and kernel-configuration catalogue (C ABI).
+ * ntt_b200 autotuner, schedules and kernel-configuration catalogue (C ABI).
  *
  * Replaces the reference's compile-time phase-triple choice
  * (DefaultNTTLaunchConfig<LogN>, src/ntt_config.h:62-73) with a run-time
@@ -12,34 +12,49 @@
 extern "C" {
 #endif
 
+/* Work distribution of a plan's transform launches (results never depend on
+ * it). */
+#define NTT_SCHEDULE_DIRECT 0 /* one limb per cluster, input from global memory  */
+#define NTT_SCHEDULE_STAGED 1 /* resident clusters, next input bulk-copied ahead */
+
 typedef struct ntt_kernel_config {
     int logN;
-    int cluster_ctas;    /* CTAs per limb (thread-block cluster size)  */
+    int cluster_ctas;    /* CTAs per limb (thread-block cluster size)    */
     int r1;              /* phase-1 (column) stages; phase 2 = logN - r1 */
-    int words_log2;      /* log2 words per thread per register pass    */
-    int k1a;             /* stages of the first phase-1 register pass   */
-    int k2a;             /* stages of the first phase-2 register pass   */
-    int threads;         /* threads per CTA                             */
-    uint32_t smem_bytes; /* dynamic shared memory per CTA               */
+    int words_log2;      /* log2 words per thread per register pass      */
+    int k1a;             /* stages of the first phase-1 register pass    */
+    int k2a;             /* stages of the first phase-2 register pass    */
+    int threads;         /* threads per CTA                              */
+    uint32_t smem_bytes; /* dynamic shared memory per CTA (direct)       */
 } ntt_kernel_config_t;
 
 typedef struct ntt_tune_result {
-    int config_index;
-    double roundtrip_us; /* forward + inverse over the timed batch      */
+    int fwd_index;  /* fastest configuration for the forward transform */
+    int inv_index;  /* ... and for the inverse                         */
+    double fwd_us;  /* its time for one launch over the timed batch    */
+    double inv_us;
     int candidates;
 } ntt_tune_result_t;
 
 NTT_API int ntt_config_count(void);
 NTT_API ntt_status_t ntt_config_get(int index, ntt_kernel_config_t* out);
+/* Thread-block clusters of configuration `index` resident at once on the
+ * current device under `schedule`; -1 on error. */
+NTT_API int ntt_config_resident_clusters(int index, int forward, int schedule);
 /* Time every compiled configuration for logN on `polys` polynomials of
- * `limbs` limbs (forward + inverse, `iters` repetitions), remember the
- * fastest for (device, logN, limb bucket) and write the on-disk cache.
- * Plans created afterwards use it when no phase split is requested. */
-NTT_API ntt_status_t ntt_autotune(int logN, int limbs, int polys, int iters, ntt_tune_result_t* out);
+ * `limbs` limbs (forward and inverse separately, `iters` launches each),
+ * remember the fastest of each direction for (device, logN, limb bucket)
+ * and write the on-disk cache.  Plans created afterwards use them when no
+ * phase split is requested. */
+NTT_API ntt_status_t ntt_autotune(int logN, int limbs, int polys, int iters,
+                                  ntt_tune_result_t* out);
 /* Pin a plan to compiled configurations (indices into the catalogue above;
  * -1 keeps the current choice).  A tuning / debugging hook: results are
  * identical for every configuration. */
 NTT_API ntt_status_t ntt_plan_force_config(ntt_plan_t* plan, int fwd_index, int inv_index);
+/* Work distribution of the plan's launches (NTT_SCHEDULE_*; default
+ * NTT_SCHEDULE_DIRECT). */
+NTT_API ntt_status_t ntt_plan_set_schedule(ntt_plan_t* plan, int schedule);
 /* Drop tuned entries for this process (plans fall back to defaults). */
 NTT_API void ntt_autotune_forget(void);
 /* Re-read the cache file on next use. */

@@ -90,7 +90,8 @@ class KernelConfig(ctypes.Structure):
 
 
 class TuneResult(ctypes.Structure):
-    _fields_ = [("config_index", ctypes.c_int), ("roundtrip_us", ctypes.c_double),
+    _fields_ = [("fwd_index", ctypes.c_int), ("inv_index", ctypes.c_int),
+                ("fwd_us", ctypes.c_double), ("inv_us", ctypes.c_double),
                 ("candidates", ctypes.c_int)]
 
 
@@ -155,6 +156,11 @@ _sig("ntt_autotune", _st, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int
      ctypes.POINTER(TuneResult))
 _sig("ntt_autotune_forget", None)
 _sig("ntt_plan_force_config", _st, _vp, ctypes.c_int, ctypes.c_int)
+_sig("ntt_plan_set_schedule", _st, _vp, ctypes.c_int)
+_sig("ntt_plan_check", _st, _vp, ctypes.POINTER(ctypes.c_uint32))
+_sig("ntt_config_resident_clusters", ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
+SCHEDULE_DIRECT = 0
+SCHEDULE_STAGED = 1
 _sig("ntt_autotune_reload", None)
 
 
@@ -295,6 +301,19 @@ class Plan:
         """Pin the plan to compiled configurations (see kernel_configs())."""
         _check(_lib.ntt_plan_force_config(self._h, fwd_index, inv_index), "ntt_plan_force_config")
 
+    def set_schedule(self, schedule: int = SCHEDULE_DIRECT):
+        """SCHEDULE_DIRECT: one limb per cluster, input from global memory;
+        SCHEDULE_STAGED: resident clusters with the next input slab
+        bulk-copied ahead.  Results do not depend on it."""
+        _check(_lib.ntt_plan_set_schedule(self._h, schedule), "ntt_plan_set_schedule")
+
+    def check(self) -> int:
+        """Synchronize, read and clear the plan's device status word; raises
+        NttError(NTT_ERR_TIMEOUT) if a bounded wait expired."""
+        st = ctypes.c_uint32()
+        _check(_lib.ntt_plan_check(self._h, ctypes.byref(st)), "ntt_plan_check")
+        return st.value
+
     def tables(self):
         """(forward pairs, inverse pairs, moduli) device addresses."""
         f, i, q = _vp(), _vp(), _vp()
@@ -363,6 +382,12 @@ def kernel_configs() -> List[KernelConfig]:
         _check(_lib.ntt_config_get(i, ctypes.byref(c)), "ntt_config_get")
         out.append(c)
     return out
+
+
+def resident_clusters(index: int, forward: bool = True, schedule: int = SCHEDULE_DIRECT) -> int:
+    """Clusters of compiled configuration `index` resident at once on the
+    current device under `schedule`."""
+    return _lib.ntt_config_resident_clusters(index, 1 if forward else 0, schedule)
 
 
 def autotune(logN: int, limbs: int, polys: int = 8, iters: int = 5) -> TuneResult:

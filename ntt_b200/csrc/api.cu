@@ -57,8 +57,24 @@ ntt_status_t cuda_fail(cudaError_t e, const char* what) {
 // ---------------------------------------------------------------------------
 namespace nttb {
 
-const FusedConfig* default_config(int logN) {
+// Untuned defaults per direction (measured on B200: the fastest direct-
+// schedule configuration for 16-limb batches larger than L2); otherwise the
+// first compiled configuration for logN.
+const FusedConfig* default_config(int logN, bool fwd) {
+    struct Pick {
+        int logN, clog, r1, eb, k1a, k2a;
+        bool fwd;
+    };
+    static const Pick picks[] = {{16, 3, 8, 5, 3, 4, true}, {16, 3, 7, 5, 3, 5, false},
+                                 {17, 4, 8, 5, 3, 5, true}, {17, 4, 8, 5, 3, 5, false},
+                                 {15, 1, 10, 5, 5, 5, false}};
     const FusedConfig* c = fused_configs();
+    for (const Pick& p : picks)
+        if (p.logN == logN && p.fwd == fwd)
+            for (int i = 0; i < fused_config_count(); ++i)
+                if (c[i].logN == p.logN && c[i].clog == p.clog && c[i].r1 == p.r1 &&
+                    c[i].eb == p.eb && c[i].k1a == p.k1a && c[i].k2a == p.k2a)
+                    return &c[i];
     for (int i = 0; i < fused_config_count(); ++i)
         if (c[i].logN == logN) return &c[i];
     return nullptr;
@@ -98,14 +114,23 @@ void effective_triples(const FusedConfig* c, int logN, TransformConfig* t) {
 static std::mutex g_attr_mu;
 static std::set<std::pair<int, const void*>> g_attr_done;
 
+static uint32_t smem_of(const FusedConfig* c, const void* fn) {
+    return (fn == c->fwd_direct || fn == c->inv_direct) ? c->smem_bytes_direct : c->smem_bytes;
+}
+
+static const void* kernel_of(const FusedConfig* c, bool fwd, int schedule) {
+    if (schedule == NTT_SCHEDULE_STAGED) return fwd ? c->fwd : c->inv;
+    return fwd ? c->fwd_direct : c->inv_direct;
+}
+
 ntt_status_t prepare_function(const FusedConfig* c, const void* fn) {
     int dev = 0;
     NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
     std::lock_guard<std::mutex> lk(g_attr_mu);
     if (g_attr_done.count({dev, fn})) return NTT_OK;
-    if (c->smem_bytes > 48 * 1024)
+    if (smem_of(c, fn) > 48 * 1024)
         NTT_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)c->smem_bytes),
+                                          (int)smem_of(c, fn)),
                      "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
     if ((1 << c->clog) > 8)
         NTT_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
@@ -114,18 +139,76 @@ ntt_status_t prepare_function(const FusedConfig* c, const void* fn) {
     return NTT_OK;
 }
 
-ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s) {
+// Resident clusters of a kernel on the current device (cached).
+static std::mutex g_occ_mu;
+static std::map<std::pair<int, const void*>, int> g_occ;
+
+static int resident_clusters(const FusedConfig* c, const void* fn) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        auto it = g_occ.find({dev, fn});
+        if (it != g_occ.end()) return it->second;
+    }
+    const unsigned C = 1u << c->clog;
+    int n = 0;
+    if (C > 1) {
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(C * 1024, 1, 1);
+        lc.blockDim = dim3((unsigned)c->threads, 1, 1);
+        lc.dynamicSmemBytes = smem_of(c, fn);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        if (cudaOccupancyMaxActiveClusters(&n, fn, &lc) != cudaSuccess) n = 0;
+    } else {
+        int per_sm = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, c->threads,
+                                                          smem_of(c, fn)) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+            n = per_sm * sms;
+    }
+    cudaGetLastError();  // clear a failed query; n = 0 falls back below
+    if (n <= 0) n = 148;
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    g_occ[{dev, fn}] = n;
+    return n;
+}
+
+int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule) {
+    const void* fn = kernel_of(c, fwd, schedule);
+    if (prepare_function(c, fn) != NTT_OK) return -1;
+    return resident_clusters(c, fn);
+}
+
+// NTT_SCHEDULE_DIRECT: one limb per cluster, input straight from global
+// memory, the hardware scheduling the clusters.  NTT_SCHEDULE_STAGED: one
+// wave of resident clusters, each running a contiguous chunk of limb-major
+// jobs with the next input slab bulk-copied ahead.
+ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
+                          int schedule) {
     if (a.jobs == 0) return NTT_OK;
-    const void* fn = fwd ? c->fwd : c->inv;
+    const void* fn = kernel_of(c, fwd, schedule);
     ntt_status_t st = prepare_function(c, fn);
     if (st != NTT_OK) return st;
     const unsigned C = 1u << c->clog;
-    if ((unsigned long long)a.jobs * C > (unsigned long long)INT_MAX)
+    uint32_t per = 1;
+    if (schedule == NTT_SCHEDULE_STAGED) {
+        const uint32_t resident = (uint32_t)resident_clusters(c, fn);
+        per = (a.jobs + resident - 1) / resident;
+    }
+    const uint32_t clusters = (a.jobs + per - 1) / per;
+    if ((unsigned long long)clusters * C > (unsigned long long)INT_MAX)
         return fail(NTT_ERR_INVALID_ARGUMENT, "too many limb transforms in one launch");
     cudaLaunchConfig_t lc = {};
-    lc.gridDim = dim3(C * a.jobs, 1, 1);
+    lc.gridDim = dim3(C * clusters, 1, 1);
     lc.blockDim = dim3((unsigned)c->threads, 1, 1);
-    lc.dynamicSmemBytes = c->smem_bytes;
+    lc.dynamicSmemBytes = smem_of(c, fn);
     lc.stream = s;
     cudaLaunchAttribute attr[1];
     if (C > 1) {
@@ -137,6 +220,7 @@ ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cu
         lc.numAttrs = 1;
     }
     FusedArgs arg = a;
+    arg.jobs_per_cluster = per;
     void* args[] = {&arg};
     NTT_CUDA_TRY(cudaLaunchKernelExC(&lc, fn, args), "fused NTT launch");
     return NTT_OK;
@@ -154,11 +238,13 @@ struct ntt_plan {
     TwPair* fwd = nullptr;
     TwPair* inv = nullptr;
     uint32_t* q = nullptr;
+    uint32_t* status = nullptr;  // device word: bit 0 = a bounded wait expired
     size_t bytes = 0;
     const FusedConfig* cfg_fwd = nullptr;  // nullptr: small kernel
     const FusedConfig* cfg_inv = nullptr;
     TransformConfig effective{};
     int tuned = 0;
+    int schedule = NTT_SCHEDULE_DIRECT;
 };
 
 namespace nttb {
@@ -210,10 +296,11 @@ ntt_status_t check_transform(int logN, const TransformConfig* t) {
 void choose_configs(ntt_plan* p, const TransformConfig* t) {
     p->cfg_fwd = p->cfg_inv = nullptr;
     if (p->logN <= kSmallMaxLogN || !default_config(p->logN)) return;
-    const FusedConfig* tuned = tuned_config(p->logN, p->limbs);
-    const FusedConfig* def = tuned ? tuned : default_config(p->logN);
-    p->tuned = tuned != nullptr;
-    p->cfg_fwd = p->cfg_inv = def;
+    const FusedConfig* tf = tuned_config(p->logN, p->limbs, true);
+    const FusedConfig* ti = tuned_config(p->logN, p->limbs, false);
+    p->tuned = (tf != nullptr) || (ti != nullptr);
+    p->cfg_fwd = tf ? tf : default_config(p->logN, true);
+    p->cfg_inv = ti ? ti : default_config(p->logN, false);
     if (t) {
         if (auto c = config_by_r1(p->logN, t->ntt_phase1.radix_stages)) p->cfg_fwd = c;
         if (auto c = config_by_r1(p->logN, t->intt_phase2.radix_stages)) p->cfg_inv = c;
@@ -333,7 +420,7 @@ ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int limbs,
     cudaError_t e = cudaGetDevice(&p->device);
     const size_t tw_bytes = (size_t)limbs * N * sizeof(TwPair);
     const size_t q_bytes = ((size_t)limbs * 4 + 255) & ~(size_t)255;
-    p->bytes = 2 * tw_bytes + q_bytes;
+    p->bytes = 2 * tw_bytes + q_bytes + 256;
     if (e == cudaSuccess) e = cudaMalloc(&p->block, p->bytes);
     TwGenLimb* gdev = nullptr;
     if (e == cudaSuccess) e = cudaMalloc(&gdev, 2 * limbs * sizeof(TwGenLimb));
@@ -341,7 +428,9 @@ ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int limbs,
         p->fwd = (TwPair*)p->block;
         p->inv = (TwPair*)((char*)p->block + tw_bytes);
         p->q = (uint32_t*)((char*)p->block + 2 * tw_bytes);
+        p->status = (uint32_t*)((char*)p->block + 2 * tw_bytes + q_bytes);
         e = cudaMemcpy(p->q, qh.data(), limbs * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(p->status, 0, 4);
     }
     if (e == cudaSuccess) e = cudaMemcpy(gdev, gf.data(), limbs * sizeof(TwGenLimb), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
@@ -388,7 +477,8 @@ ntt_status_t ntt_plan_get_info(const ntt_plan_t* p, ntt_plan_info_t* out) {
     const FusedConfig* c = p->cfg_fwd;
     out->cluster_ctas = c ? (1 << c->clog) : 1;
     out->threads_per_cta = c ? c->threads : ((1 << (p->logN - 1)) < 32 ? 32 : (1 << (p->logN - 1)));
-    out->smem_bytes = c ? c->smem_bytes : (4u << p->logN);
+    out->smem_bytes = c ? (p->schedule == NTT_SCHEDULE_STAGED ? c->smem_bytes : c->smem_bytes_direct)
+                        : (4u << p->logN);
     out->effective = p->effective;
     out->device_bytes = p->bytes;
     out->tuned = p->tuned;
@@ -412,6 +502,25 @@ ntt_status_t ntt_plan_force_config(ntt_plan_t* p, int fwd_index, int inv_index) 
     return NTT_OK;
 }
 
+ntt_status_t ntt_plan_check(const ntt_plan_t* p, uint32_t* device_status) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    uint32_t st = 0;
+    NTT_CUDA_TRY(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    NTT_CUDA_TRY(cudaMemcpy(&st, p->status, 4, cudaMemcpyDeviceToHost), "status read");
+    NTT_CUDA_TRY(cudaMemset(p->status, 0, 4), "status reset");
+    if (device_status) *device_status = st;
+    if (st & 1u) return fail(NTT_ERR_TIMEOUT, "a bounded wait in a transform kernel expired");
+    return NTT_OK;
+}
+
+ntt_status_t ntt_plan_set_schedule(ntt_plan_t* p, int schedule) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    if (schedule != NTT_SCHEDULE_DIRECT && schedule != NTT_SCHEDULE_STAGED)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "unknown schedule %d", schedule);
+    p->schedule = schedule;
+    return NTT_OK;
+}
+
 ntt_status_t ntt_plan_tables(const ntt_plan_t* p, const uint32_t** fwd, const uint32_t** inv,
                              const uint32_t** q) {
     if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
@@ -430,7 +539,7 @@ namespace nttb {
 
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
-                           cudaStream_t s) {
+                           cudaStream_t s, uint32_t* status, int schedule) {
     if (polys == 0) return NTT_OK;
     if (!a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL data pointer");
     // the fused kernels move 16-byte vectors; the small-size kernel words
@@ -444,8 +553,9 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
     const size_t jobs = polys * (size_t)limbs;
     if (jobs > (size_t)UINT_MAX) return fail(NTT_ERR_INVALID_ARGUMENT, "too many limbs");
     if (cfg) {
-        FusedArgs fa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride};
-        return launch_fused(cfg, fwd, fa, s);
+        FusedArgs fa{a,  tw, q, (uint32_t)limbs, (uint32_t)polys, (uint32_t)jobs, 1u,
+                     (unsigned long long)stride, status};
+        return launch_fused(cfg, fwd, fa, s, schedule);
     }
     SmallArgs sa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride, logN};
     NTT_CUDA_TRY(launch_small(sa, fwd, s), "small NTT launch");
@@ -462,7 +572,8 @@ static ntt_status_t plan_run(const ntt_plan_t* p, uint32_t* a, size_t polys, siz
                     p->device, dev);
     if (stride == 0) stride = (size_t)p->limbs << p->logN;
     return run_transform(p->logN, fwd ? p->cfg_fwd : p->cfg_inv, fwd ? p->fwd : p->inv, p->q,
-                         p->limbs, a, polys, stride, fwd, (cudaStream_t)s);
+                         p->limbs, a, polys, stride, fwd, (cudaStream_t)s, p->status,
+                         p->schedule);
 }
 
 }  // namespace nttb
@@ -547,10 +658,11 @@ ntt_status_t shim_run(uint32_t* A, const uint32_t* tw, const uint32_t* moduli, c
         // column stages: NTT phase 1 / INTT phase 2 (the second triple)
         const PhaseConfig* col = inverse ? ph2 : ph1;
         cfg = col ? config_by_r1(logN, col->radix_stages) : nullptr;
-        if (!cfg) cfg = tuned_config(logN, (int)limbs);
-        if (!cfg) cfg = default_config(logN);
+        if (!cfg) cfg = tuned_config(logN, (int)limbs, !inverse);
+        if (!cfg) cfg = default_config(logN, !inverse);
     }
-    return run_transform(logN, cfg, table, moduli, (int)limbs, A, 1, limbs << logN, !inverse, 0);
+    return run_transform(logN, cfg, table, moduli, (int)limbs, A, 1, limbs << logN, !inverse, 0,
+                         nullptr, NTT_SCHEDULE_DIRECT);
 }
 }  // namespace
 

@@ -34,9 +34,12 @@ namespace nttb {
 struct FusedConfig {
     int logN, clog, r1, eb, k1a, k2a;
     int threads;
-    uint32_t smem_bytes;
-    const void* fwd;  // __global__ fused_kernel<G, true>
-    const void* inv;  // __global__ fused_kernel<G, false>
+    uint32_t smem_bytes;         // staged kernels (work + stage buffer + mbarrier)
+    uint32_t smem_bytes_direct;  // direct kernels (work buffer)
+    const void* fwd;             // fused_kernel<G, true,  true>  (staged)
+    const void* inv;             // fused_kernel<G, false, true>
+    const void* fwd_direct;      // fused_kernel<G, true,  false> (direct)
+    const void* inv_direct;      // fused_kernel<G, false, false>
 };
 
 // All compiled configurations (registry.cu); count via fused_config_count().

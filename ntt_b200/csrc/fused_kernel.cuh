@@ -5,17 +5,27 @@
 
 namespace nttb {
 
-// Arguments of one launch over `jobs` limb transforms of one plan.
-// Job j is limb (j % limbs) of polynomial (j / limbs); polynomial p starts
-// at data + p * poly_stride (words), limb l at + l * N.
+// Arguments of one launch over `jobs` = polys * limbs limb transforms of one
+// plan.  Jobs are numbered limb-major (job j: limb j / polys, polynomial
+// j % polys) so that consecutive jobs share a modulus and its twiddles;
+// cluster c runs jobs [c * jobs_per_cluster, (c+1) * jobs_per_cluster).
+// Polynomial p starts at data + p * poly_stride (words), limb l at + l * N.
 struct FusedArgs {
     uint32_t* data;
-    const TwPair* tw;      // [limbs][N] forward or inverse table (see twiddle.cu)
-    const uint32_t* q;     // [limbs]
+    const TwPair* tw;   // [limbs][N] forward or inverse table (see twiddle.cu)
+    const uint32_t* q;  // [limbs]
     uint32_t limbs;
+    uint32_t polys;
     uint32_t jobs;
+    uint32_t jobs_per_cluster;
     unsigned long long poly_stride;
+    uint32_t* status;  // optional: bit 0 set when a bounded wait expired
 };
+
+// Iteration bound of every mbarrier wait (each try_wait itself blocks for a
+// hardware-defined interval); expiry sets the status bit instead of hanging.
+constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr uint32_t kStatusWaitExpired = 1u;
 
 __device__ __forceinline__ uint32_t cluster_rank() {
     uint32_t r;
@@ -25,58 +35,155 @@ __device__ __forceinline__ uint32_t cluster_rank() {
 __device__ __forceinline__ void cluster_arrive_release() {
     asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void cluster_arrive_relaxed() {
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
 __device__ __forceinline__ void cluster_wait_acquire() {
     asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void mbar_init(uint32_t sa, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t sa, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sa), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t sa, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(sa), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false when kWaitLimit tries expired.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t sa, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitLimit; ++i)
+        if (mbar_try_wait(sa, parity)) return true;
+    return false;
+}
+// Generic-proxy accesses of shared memory before async-proxy writes to it.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// Bulk (non-tensor, non-multicast) copy global -> this CTA's shared memory.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst_sa, const void* src, uint32_t bytes,
+                                         uint32_t mbar_sa) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+        "[%3];" ::"r"(dst_sa),
+        "l"(src), "r"(bytes), "r"(mbar_sa)
+        : "memory");
+}
 
-template <int C>
+// Memory interface used by the pass code (ntt_core.cuh): every access is a
+// per-thread base plus a compile-time offset, which the compiler turns into
+// an immediate address offset.
+template <int C, bool Staged>
 struct DevCtx {
+    static constexpr bool kStaged = Staged;
     uint32_t* __restrict__ g;
     const TwPair* __restrict__ twp;
     uint32_t* smem;
-    uint32_t smem_sa;  // .shared window address of smem
+    const uint32_t* stage;  // padded copy of this CTA's input slab (staged)
+    uint32_t smem_sa;       // .shared window address of smem
     uint32_t q, q2, rank;
 
-    __device__ __forceinline__ uint32_t gload(uint32_t o) const {
-        uint32_t v;
-        asm volatile("ld.global.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(g + o));
-        return v;
+    // global data (direct input): L1-cached, because a thread owning a
+    // contiguous run reads each 32-byte sector in two 16-byte halves
+    __device__ __forceinline__ uint32_t* g_base(uint32_t o) const { return g + o; }
+    __device__ __forceinline__ uint32_t g_ld(const uint32_t* b, uint32_t c) const {
+        return __ldca(b + c);
     }
-    __device__ __forceinline__ void gload4(uint32_t o, uint32_t& a, uint32_t& b, uint32_t& c,
-                                           uint32_t& d) const {
-        asm volatile("ld.global.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
-                     : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
-                     : "l"(g + o));
+    __device__ __forceinline__ void g_ld4(const uint32_t* b, uint32_t c, uint32_t& x, uint32_t& y,
+                                          uint32_t& z, uint32_t& w) const {
+        const uint4 t = __ldca(reinterpret_cast<const uint4*>(b + c));
+        x = t.x;
+        y = t.y;
+        z = t.z;
+        w = t.w;
     }
-    __device__ __forceinline__ void gstore(uint32_t o, uint32_t v) const { g[o] = v; }
-    __device__ __forceinline__ void gstore4(uint32_t o, uint32_t a, uint32_t b, uint32_t c,
-                                            uint32_t d) const {
-        *reinterpret_cast<uint4*>(g + o) = make_uint4(a, b, c, d);
+    __device__ __forceinline__ void g_st(uint32_t* b, uint32_t c, uint32_t v) const { b[c] = v; }
+    __device__ __forceinline__ void g_st4(uint32_t* b, uint32_t c, uint32_t x, uint32_t y,
+                                          uint32_t z, uint32_t w) const {
+        *reinterpret_cast<uint4*>(b + c) = make_uint4(x, y, z, w);
     }
-    __device__ __forceinline__ uint32_t sload(uint32_t w) const { return smem[w]; }
-    __device__ __forceinline__ void sstore(uint32_t w, uint32_t v) const { smem[w] = v; }
-    __device__ __forceinline__ void rstore(uint32_t dst, uint32_t w, uint32_t v) const {
+    // stage buffer
+    __device__ __forceinline__ const uint32_t* st_base(uint32_t w) const { return stage + w; }
+    __device__ __forceinline__ uint32_t st_ld(const uint32_t* b, uint32_t c) const { return b[c]; }
+    __device__ __forceinline__ void st_ld4(const uint32_t* b, uint32_t c, uint32_t& x, uint32_t& y,
+                                           uint32_t& z, uint32_t& w) const {
+        const uint4 t = *reinterpret_cast<const uint4*>(b + c);
+        x = t.x;
+        y = t.y;
+        z = t.z;
+        w = t.w;
+    }
+    // local shared memory (work buffer)
+    __device__ __forceinline__ uint32_t* s_base(uint32_t w) const { return smem + w; }
+    __device__ __forceinline__ uint32_t s_ld(const uint32_t* b, uint32_t c) const { return b[c]; }
+    __device__ __forceinline__ void s_st(uint32_t* b, uint32_t c, uint32_t v) const { b[c] = v; }
+    // scatter target: the owner CTA's work buffer (DSMEM address when C > 1)
+    __device__ __forceinline__ auto r_base(uint32_t dst, uint32_t w) const {
         if constexpr (C == 1) {
-            smem[w] = v;
+            return smem + w;
         } else {
             uint32_t ra;
-            asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(smem_sa), "r"(dst));
-            asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(ra + 4u * w), "r"(v)
+            asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(smem_sa + 4u * w), "r"(dst));
+            return ra;
+        }
+    }
+    template <uint32_t Off, class B>
+    __device__ __forceinline__ void r_st(B rb, uint32_t v) const {
+        if constexpr (C == 1) {
+            rb[Off] = v;
+        } else {
+            asm volatile("st.shared::cluster.u32 [%0+%2], %1;" ::"r"(rb), "r"(v), "n"(Off * 4u)
                          : "memory");
         }
     }
-    __device__ __forceinline__ TwPair tw(uint32_t i) const {
-        uint2 t = __ldg(reinterpret_cast<const uint2*>(twp) + i);
+    // twiddles: re-read by every limb with this modulus (read-only cache)
+    __device__ __forceinline__ TwPair tw_at(uint32_t i) const {
+        const uint2 t = __ldg(reinterpret_cast<const uint2*>(twp) + i);
         return TwPair{t.x, t.y};
     }
+    __device__ __forceinline__ const TwPair* tw_base(uint32_t i) const { return twp + i; }
+    __device__ __forceinline__ TwPair tw_ld(const TwPair* b, uint32_t c) const {
+        const uint2 t = __ldg(reinterpret_cast<const uint2*>(b + c));
+        return TwPair{t.x, t.y};
+    }
+    __device__ __forceinline__ void tw_ld2(const TwPair* b, uint32_t c, TwPair& x,
+                                           TwPair& y) const {
+        const uint4 t = __ldg(reinterpret_cast<const uint4*>(b + c));
+        x = TwPair{t.x, t.y};
+        y = TwPair{t.z, t.w};
+    }
+    // Every loaded word has been consumed by register arithmetic when this is
+    // called, so a relaxed arrive is enough to order those reads before the
+    // peers' scatter into this CTA.
     __device__ __forceinline__ void after_local_reads() const {
-        if constexpr (C > 1) cluster_arrive_release();
+        if constexpr (C > 1) cluster_arrive_relaxed();
     }
     __device__ __forceinline__ void before_scatter() const {
         if constexpr (C > 1) cluster_wait_acquire();
     }
 };
 
+// Exchange between two register passes of one phase: a warp barrier when
+// each warp owns the same elements in both passes.
+template <bool WarpLocal>
+__device__ __forceinline__ void pass_sync() {
+    if constexpr (WarpLocal) __syncwarp();
+    else __syncthreads();
+}
+
+// Phase boundary: after the scatter, every scattered word must be visible
+// to its owner before phase 2 (forward) / phase 1 (inverse) reads it.
 template <class G>
 __device__ __forceinline__ void cta_or_cluster_sync() {
     if constexpr (G::C > 1) {
@@ -87,62 +194,108 @@ __device__ __forceinline__ void cta_or_cluster_sync() {
     }
 }
 
-template <class G, class Arith>
-__device__ __forceinline__ void fused_forward_body(DevCtx<G::C>& ctx) {
-    using F = Forward<G, Arith, DevCtx<G::C>>;
+// Issue the bulk copies of job `job`'s input slab into the stage buffer
+// (called by every thread once the whole CTA has read the previous slab).
+template <class G, bool Fwd>
+__device__ __forceinline__ void issue_slab(const FusedArgs& a, uint32_t job, uint32_t rank,
+                                           uint32_t stage_sa, uint32_t mbar_sa) {
+    const uint32_t limb = job / a.polys, poly = job - limb * a.polys;
+    const uint32_t* src = a.data + (size_t)poly * a.poly_stride + ((size_t)limb << G::LOGN);
+    fence_proxy_async_smem();
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar_sa, G::M * 4u);
+    for (uint32_t i = threadIdx.x; i < slab_copies<G, Fwd>(); i += G::THREADS) {
+        const SlabCopy c = slab_copy<G, Fwd>(rank, i);
+        bulk_g2s(stage_sa + 4u * c.dst, src + c.src, 4u * c.words, mbar_sa);
+    }
+}
+
+// One limb transform; `prefetch()` is called once the stage buffer is free.
+template <class G, bool Staged, class Arith, class Pre>
+__device__ __forceinline__ void fused_forward_body(DevCtx<G::C, Staged>& ctx, Pre&& prefetch) {
+    using F = Forward<G, Arith, DevCtx<G::C, Staged>>;
     const uint32_t tid = threadIdx.x;
     F::pass1a(ctx, tid);
     if constexpr (G::K1B > 0) {
-        __syncthreads();
+        pass_sync<G::WARP1>();
         F::pass1b(ctx, tid);
     }
     cta_or_cluster_sync<G>();
+    prefetch();  // every warp has read the stage buffer
     F::pass2a(ctx, tid);
     if constexpr (G::K2B > 0) {
-        __syncthreads();
+        pass_sync<G::WARP2>();
         F::pass2b(ctx, tid);
     }
 }
 
-template <class G, class Arith>
-__device__ __forceinline__ void fused_inverse_body(DevCtx<G::C>& ctx) {
-    using I = Inverse<G, Arith, DevCtx<G::C>>;
+template <class G, bool Staged, class Arith, class Pre>
+__device__ __forceinline__ void fused_inverse_body(DevCtx<G::C, Staged>& ctx, Pre&& prefetch) {
+    using I = Inverse<G, Arith, DevCtx<G::C, Staged>>;
     const uint32_t tid = threadIdx.x;
     if constexpr (G::K2B > 0) {
         I::pass2b(ctx, tid);
-        __syncthreads();
+        pass_sync<G::WARP2>();
     }
     I::pass2a(ctx, tid);
     cta_or_cluster_sync<G>();
+    prefetch();  // every warp has read the stage buffer
     if constexpr (G::K1B > 0) {
         I::pass1b(ctx, tid);
-        __syncthreads();
+        pass_sync<G::WARP1>();
     }
     I::pass1a(ctx, tid);
 }
 
-// One cluster of G::C CTAs per limb transform; grid.x = C * jobs.
-template <class G, bool Fwd>
-__global__ void __launch_bounds__(G::THREADS) fused_kernel(FusedArgs a) {
+// Each cluster of G::C CTAs runs a contiguous chunk of limb-major jobs
+// [j0, j1).  Staged: the CTA's input slab is bulk-copied into the stage
+// buffer one job ahead (mbarrier-tracked, bounded waits); otherwise the
+// first pass loads straight from global memory.  grid.x = C * clusters.
+template <class G, bool Fwd, bool Staged>
+__global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedArgs a) {
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t rank = (G::C > 1) ? cluster_rank() : 0u;
-    const uint32_t job = blockIdx.x / G::C;
-    const uint32_t limb = job % a.limbs;
-    const uint32_t poly = job / a.limbs;
-    DevCtx<G::C> ctx;
-    ctx.g = a.data + (size_t)poly * a.poly_stride + ((size_t)limb << G::LOGN);
-    ctx.twp = a.tw + ((size_t)limb << G::LOGN);
+    const uint32_t cluster = blockIdx.x / G::C;
+    const uint32_t j0 = cluster * a.jobs_per_cluster;
+    const uint32_t j1 = min(j0 + a.jobs_per_cluster, a.jobs);
+    const uint32_t smem_sa = (uint32_t)__cvta_generic_to_shared(smem);
+    const uint32_t stage_sa = smem_sa + 4u * G::STAGE_OFF_WORDS;
+    const uint32_t mbar_sa = smem_sa + 4u * G::MBAR_OFF_WORDS;
+    if constexpr (Staged) {
+        if (threadIdx.x == 0) {
+            mbar_init(mbar_sa, 1);
+            fence_mbar_init();
+        }
+        __syncthreads();
+        if (j0 < j1) issue_slab<G, Fwd>(a, j0, rank, stage_sa, mbar_sa);
+    }
+    DevCtx<G::C, Staged> ctx;
     ctx.smem = smem;
-    ctx.smem_sa = (uint32_t)__cvta_generic_to_shared(smem);
-    ctx.q = __ldg(a.q + limb);
-    ctx.q2 = 2u * ctx.q;
+    ctx.stage = smem + G::STAGE_OFF_WORDS;
+    ctx.smem_sa = smem_sa;
     ctx.rank = rank;
-    if (ctx.q < (1u << 30)) {
-        if constexpr (Fwd) fused_forward_body<G, Lazy4>(ctx);
-        else fused_inverse_body<G, Lazy4>(ctx);
-    } else {
-        if constexpr (Fwd) fused_forward_body<G, Lazy2>(ctx);
-        else fused_inverse_body<G, Lazy2>(ctx);
+    uint32_t parity = 0;
+    for (uint32_t job = j0; job < j1; ++job, parity ^= 1u) {
+        const uint32_t limb = job / a.polys, poly = job - limb * a.polys;
+        ctx.g = a.data + (size_t)poly * a.poly_stride + ((size_t)limb << G::LOGN);
+        ctx.twp = a.tw + ((size_t)limb << G::LOGN);
+        ctx.q = __ldg(a.q + limb);
+        ctx.q2 = 2u * ctx.q;
+        if constexpr (Staged) {
+            if (!mbar_wait_bounded(mbar_sa, parity) && a.status)
+                atomicOr(a.status, kStatusWaitExpired);
+        }
+        auto prefetch = [&]() {
+            if constexpr (Staged)
+                if (job + 1 < j1) issue_slab<G, Fwd>(a, job + 1, rank, stage_sa, mbar_sa);
+        };
+        if (ctx.q < (1u << 30)) {
+            if constexpr (Fwd) fused_forward_body<G, Staged, Lazy4>(ctx, prefetch);
+            else fused_inverse_body<G, Staged, Lazy4>(ctx, prefetch);
+        } else {
+            if constexpr (Fwd) fused_forward_body<G, Staged, Lazy2>(ctx, prefetch);
+            else fused_inverse_body<G, Staged, Lazy2>(ctx, prefetch);
+        }
+        __syncthreads();  // the work buffer is rewritten by the next job
     }
 }
 

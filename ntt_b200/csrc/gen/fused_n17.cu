@@ -3,11 +3,15 @@
 #include "../fused_kernel.cuh"
 
 namespace nttb {
-#define NTTB_ENTRY(N, CL, R1, EB, K1A, K2A)                                                  \
-    {N, CL, R1, EB, K1A, K2A, Geometry<N, CL, R1, EB, K1A, K2A>::THREADS,                   \
-     Geometry<N, CL, R1, EB, K1A, K2A>::SMEM_BYTES,                                         \
-     (const void*)&fused_kernel<Geometry<N, CL, R1, EB, K1A, K2A>, true>,                   \
-     (const void*)&fused_kernel<Geometry<N, CL, R1, EB, K1A, K2A>, false>},
+#define NTTB_G(N, CL, R1, EB, K1A, K2A) Geometry<N, CL, R1, EB, K1A, K2A>
+#define NTTB_ENTRY(N, CL, R1, EB, K1A, K2A)                                                   \
+    {N, CL, R1, EB, K1A, K2A, NTTB_G(N, CL, R1, EB, K1A, K2A)::THREADS,                      \
+     NTTB_G(N, CL, R1, EB, K1A, K2A)::SMEM_BYTES,                                            \
+     NTTB_G(N, CL, R1, EB, K1A, K2A)::SMEM_BYTES_DIRECT,                                     \
+     (const void*)&fused_kernel<NTTB_G(N, CL, R1, EB, K1A, K2A), true, true>,                \
+     (const void*)&fused_kernel<NTTB_G(N, CL, R1, EB, K1A, K2A), false, true>,               \
+     (const void*)&fused_kernel<NTTB_G(N, CL, R1, EB, K1A, K2A), true, false>,               \
+     (const void*)&fused_kernel<NTTB_G(N, CL, R1, EB, K1A, K2A), false, false>},
 extern const FusedConfig kFusedN17[] = {NTTB_CFG_N17(NTTB_ENTRY)};
 extern const int kFusedN17Count = sizeof(kFusedN17) / sizeof(kFusedN17[0]);
 }  // namespace nttb

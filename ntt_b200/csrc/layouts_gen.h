@@ -1,0 +1,148 @@
+// GENERATED by gen_layouts.py from configs.h -- do not edit.
+// Per configuration: the work-buffer bank-spreading layout (A1, C1, A2, C2,
+// size in words) and the lane masks the search assumed (checked against
+// PassLayout by static_assert in ntt_core.cuh).
+#pragma once
+#include <cstdint>
+
+namespace nttb {
+
+template <int N, int CL, int R1, int EB, int K1A, int K2A>
+struct LayoutTable;
+
+template <>
+struct LayoutTable<10, 0, 5, 5, 5, 5> {
+    static constexpr int XW[5] = {5, 16, 6, 1, 1535};
+    static constexpr uint32_t lanes_P1A = 0x1fu;
+    static constexpr uint32_t lanes_P1B = 0x3d0u;
+    static constexpr uint32_t lanes_P2A = 0x3e0u;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<11, 0, 6, 5, 1, 5> {
+    static constexpr int XW[5] = {5, 1, 11, 0, 2111};
+    static constexpr uint32_t lanes_P1A = 0x1f0u;
+    static constexpr uint32_t lanes_P1B = 0x1fu;
+    static constexpr uint32_t lanes_P2A = 0x3e0u;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<12, 0, 7, 5, 3, 5> {
+    static constexpr int XW[5] = {6, 1, 12, 0, 4159};
+    static constexpr uint32_t lanes_P1A = 0x7cu;
+    static constexpr uint32_t lanes_P1B = 0x21eu;
+    static constexpr uint32_t lanes_P2A = 0x3e0u;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<13, 0, 8, 5, 3, 5> {
+    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
+    static constexpr uint32_t lanes_P1A = 0x7cu;
+    static constexpr uint32_t lanes_P1B = 0x1fu;
+    static constexpr uint32_t lanes_P2A = 0x3e0u;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<14, 0, 9, 5, 4, 5> {
+    static constexpr int XW[5] = {5, 1, 14, 0, 16895};
+    static constexpr uint32_t lanes_P1A = 0x3eu;
+    static constexpr uint32_t lanes_P1B = 0x1fu;
+    static constexpr uint32_t lanes_P2A = 0x3e0u;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<14, 1, 9, 5, 4, 5> {
+    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
+    static constexpr uint32_t lanes_P1A = 0x3eu;
+    static constexpr uint32_t lanes_P1B = 0x20fu;
+    static constexpr uint32_t lanes_P2A = 0x3e0u;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<15, 1, 10, 5, 5, 5> {
+    static constexpr int XW[5] = {5, 1, 14, 0, 16895};
+    static constexpr uint32_t lanes_P1A = 0x1fu;
+    static constexpr uint32_t lanes_P1B = 0x20fu;
+    static constexpr uint32_t lanes_P2A = 0x3e0u;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<15, 2, 8, 5, 3, 4> {
+    static constexpr int XW[5] = {6, 1, 8, 1, 8350};
+    static constexpr uint32_t lanes_P1A = 0x7cu;
+    static constexpr uint32_t lanes_P1B = 0x1fu;
+    static constexpr uint32_t lanes_P2A = 0x386u;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<16, 3, 8, 5, 3, 4> {
+    static constexpr int XW[5] = {6, 1, 9, 1, 8334};
+    static constexpr uint32_t lanes_P1A = 0x7cu;
+    static constexpr uint32_t lanes_P1B = 0x1fu;
+    static constexpr uint32_t lanes_P2A = 0x30eu;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<16, 3, 7, 5, 3, 5> {
+    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
+    static constexpr uint32_t lanes_P1A = 0x7cu;
+    static constexpr uint32_t lanes_P1B = 0x3eu;
+    static constexpr uint32_t lanes_P2A = 0x20fu;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<16, 2, 8, 5, 3, 4> {
+    static constexpr int XW[5] = {6, 1, 9, 1, 16670};
+    static constexpr uint32_t lanes_P1A = 0x7cu;
+    static constexpr uint32_t lanes_P1B = 0x1fu;
+    static constexpr uint32_t lanes_P2A = 0x30eu;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<16, 4, 8, 5, 3, 4> {
+    static constexpr int XW[5] = {6, 1, 9, 1, 4166};
+    static constexpr uint32_t lanes_P1A = 0x7cu;
+    static constexpr uint32_t lanes_P1B = 0x20fu;
+    static constexpr uint32_t lanes_P2A = 0x30eu;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<16, 3, 8, 4, 4, 4> {
+    static constexpr int XW[5] = {6, 1, 13, 0, 8319};
+    static constexpr uint32_t lanes_P1A = 0x1fu;
+    static constexpr uint32_t lanes_P1B = 0x1fu;
+    static constexpr uint32_t lanes_P2A = 0x10fu;
+    static constexpr uint32_t lanes_P2B = 0x1f0u;
+};
+
+template <>
+struct LayoutTable<17, 3, 8, 5, 3, 5> {
+    static constexpr int XW[5] = {5, 1, 14, 0, 16895};
+    static constexpr uint32_t lanes_P1A = 0x7cu;
+    static constexpr uint32_t lanes_P1B = 0x1fu;
+    static constexpr uint32_t lanes_P2A = 0x20fu;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<17, 4, 8, 5, 3, 5> {
+    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
+    static constexpr uint32_t lanes_P1A = 0x7cu;
+    static constexpr uint32_t lanes_P1B = 0x1fu;
+    static constexpr uint32_t lanes_P2A = 0x20fu;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+}  // namespace nttb

@@ -22,33 +22,62 @@
 // words, runs KB <= EB radix-2 stages on them in registers, and stores them
 // back.  A pass is described at compile time by the bit positions of the
 // CTA-local index lambda that it owns (PassLayout): the KB butterfly bits
-// [PLO, PLO+KB), plus EB-KB "extra" bits (the lowest positions outside the
-// butterfly range, so each thread's words form contiguous runs for 128-bit
-// global access), the remaining bits being the thread index.  All index maps
-// below are linear over disjoint bit sets, so every per-register address is a
-// per-thread base plus a compile-time constant.
+// [PLO, PLO+KB), plus EB-KB "extra" bits (the lowest free positions, so each
+// thread's words form contiguous runs for 128-bit accesses), the remaining
+// bits being the lane and warp index.  All index maps below are linear over
+// disjoint bit sets, so every per-register address is a per-thread base plus
+// a compile-time constant, and every loop over registers, stages and groups
+// is a compile-time loop (ct_for), so no index arithmetic runs per element.
 #pragma once
+#include <type_traits>
+#include <utility>
+
 #include "arith.cuh"
+#include "layouts_gen.h"
 
 namespace nttb {
 
 // ---------------------------------------------------------------------------
-// Compile-time layout of one register pass.
+// Compile-time loops: f(std::integral_constant<int, I>) for I = 0..N-1.
 // ---------------------------------------------------------------------------
-template <int MB_, int PLO_, int KB_, int EB_>
+template <class F, int... Is>
+NTT_HD void ct_for_impl(F&& f, std::integer_sequence<int, Is...>) {
+    (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, class F>
+NTT_HD void ct_for(F&& f) {
+    ct_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+constexpr int popcount32(uint32_t x) {
+    int c = 0;
+    for (; x; x &= x - 1u) ++c;
+    return c;
+}
+
+// ---------------------------------------------------------------------------
+// Compile-time layout of one register pass.
+// WM: lambda positions of the warp index (0 = no constraint: the thread
+// index fills all non-register positions in ascending order).  Two passes
+// with the same WM give every warp the same element set, so the exchange
+// between them needs only a warp barrier.
+// ---------------------------------------------------------------------------
+template <int MB_, int PLO_, int KB_, int EB_, uint32_t WM_ = 0>
 struct PassLayout {
     static constexpr int MB = MB_, PLO = PLO_, KB = KB_, EB = EB_;
+    static constexpr uint32_t WM = WM_;
     static constexpr int XB = EB - KB;
     static constexpr int E = 1 << EB;
     static_assert(KB >= 1 && KB <= EB && EB <= MB, "bad pass layout");
     static_assert(PLO >= 0 && PLO + KB <= MB, "bad pass layout");
 
     static constexpr bool in_bfly(int p) { return p >= PLO && p < PLO + KB; }
-    // j-th extra position: the XB lowest positions outside the butterfly range.
+    // j-th extra position: the XB lowest positions outside the butterfly
+    // range and the warp positions.
     static constexpr int xpos(int j) {
         int cnt = 0;
         for (int p = 0; p < MB; ++p) {
-            if (in_bfly(p)) continue;
+            if (in_bfly(p) || ((WM >> p) & 1u)) continue;
             if (cnt == j) return p;
             ++cnt;
         }
@@ -86,15 +115,67 @@ struct PassLayout {
             if (xpos(j) > PLO + KB - 1) ++c;
         return c;
     }
-    // Deposit the thread index into the non-register positions (ascending).
-    NTT_HD static uint32_t dep(uint32_t t) {
-        uint32_t v = t;
-#pragma unroll
-        for (int p = 0; p < MB; ++p) {
-            if ((reg_mask() >> p) & 1u) v = ((v >> p) << (p + 1)) | (v & ((1u << p) - 1u));
-        }
+    static constexpr uint32_t kRegMask = reg_mask();
+    static_assert((kRegMask & WM) == 0, "warp positions overlap register positions");
+    static constexpr int kRunBits = run_bits();
+    static constexpr int kXHB = xhi_bits();
+    static constexpr uint32_t kFull = (MB >= 32) ? 0xFFFFFFFFu : ((1u << MB) - 1u);
+    static constexpr uint32_t kLaneMask = kFull & ~kRegMask & ~WM;
+    // the 5 lambda positions that hold the lane index (tid bits 0..4)
+    static constexpr uint32_t lanes() {
+        uint32_t m = (WM == 0) ? (kFull & ~kRegMask) : kLaneMask, out = 0;
+        for (int p = 0, c = 0; p < MB && c < 5; ++p)
+            if ((m >> p) & 1u) {
+                out |= 1u << p;
+                ++c;
+            }
+        return out;
+    }
+    static constexpr uint32_t kLanes = lanes();
+    // Deposit the bits of x into the set positions of Mask (ascending).
+    template <uint32_t Mask>
+    NTT_HD static uint32_t deposit(uint32_t x) {
+        uint32_t v = 0;
+        ct_for<MB>([&](auto P) {
+            constexpr int p = decltype(P)::value;
+            if constexpr (((Mask >> p) & 1u) != 0) {
+                constexpr int rank = popcount32(Mask & ((1u << p) - 1u));
+                v |= ((x >> rank) & 1u) << p;
+            }
+        });
         return v;
     }
+    // lambda bits owned by thread t (its register offsets are added to this)
+    NTT_HD static uint32_t dep(uint32_t t) {
+        if constexpr (WM == 0) {
+            return deposit<kFull & ~kRegMask>(t);
+        } else {
+            return deposit<kLaneMask>(t & 31u) | deposit<WM>(t >> 5);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Shared-memory layouts.  The work buffer uses one bank-spreading layout
+//     phys(l) = l + C1 * (l >> A1) + C2 * (l >> A2)
+// per configuration, which is monotone (so injective) and additive over
+// disjoint bit sets (so a thread's addresses stay base + compile-time
+// offset).  It is the same for every pass because each pass rewrites, in
+// place, exactly the words it read.  A1..C2 are chosen offline by
+// gen_layouts.py (layouts_gen.h) to minimise warp-wide bank conflicts of all
+// the passes' lane patterns.
+// ---------------------------------------------------------------------------
+template <int A1, int C1, int A2, int C2>
+struct Spread {
+    static constexpr uint32_t phys(uint32_t l) {
+        return l + (uint32_t)C1 * (l >> A1) + (uint32_t)C2 * (l >> A2);
+    }
+};
+
+// Stage buffer: one 16-byte pad per 128 bytes (conflict-free 128-bit reads
+// whether a thread's run starts every 32 words or every row).
+struct StageLayout {
+    static constexpr uint32_t phys(uint32_t l) { return l + 4u * (l >> 5); }
 };
 
 // ---------------------------------------------------------------------------
@@ -115,25 +196,82 @@ struct Geometry {
     static constexpr uint32_t H2 = 1u << (R1 - CLOG);
     static constexpr int TB = MB - EB;
     static constexpr int THREADS = 1 << TB;
+    // Register budget: the transforms are latency-bound, so ask for enough
+    // resident CTAs that each thread keeps at most 64 registers.
+    static constexpr int MIN_BLOCKS =
+        (65536 / (THREADS * 64)) > 0 ? (65536 / (THREADS * 64)) : 1;
     static constexpr int K1A = K1A_, K1B = R1 - K1A_;
     static constexpr int K2A = K2A_, K2B = R2 - K2A_;
     static_assert(R1 >= CLOG && R2 >= CLOG, "each phase needs at least c stages");
     static_assert(K1A >= 1 && K1A <= EB && K1B >= 0 && K1B <= EB, "phase-1 passes");
     static_assert(K2A >= 1 && K2A <= EB && K2B >= 0 && K2B <= EB, "phase-2 passes");
     static_assert(TB >= 5 && TB <= 10, "32..1024 threads per CTA");
-    // Padded shared-memory layout: one pad word per 32 (bank spreading).
-    static constexpr uint32_t SMEM_WORDS = M + (M >> 5);
-    static constexpr uint32_t SMEM_BYTES = SMEM_WORDS * 4u;
+
+    // Bulk copies of the input slab in pieces of COPY_WORDS (<= 128 bytes, so
+    // a piece never straddles a stage pad): forward = each phase-1 row's W1
+    // words owned by this CTA; inverse = the contiguous phase-2 slab.
+    static constexpr uint32_t COPY_WORDS = W1 < 32u ? W1 : 32u;
+    static constexpr uint32_t FWD_COPIES = (1u << R1) * (W1 / COPY_WORDS);
+    static constexpr uint32_t INV_COPIES = M / 32u;
+    static constexpr uint32_t STAGE_WORDS = StageLayout::phys(M - 1u) + 1u;
+
+    // Warp ownership.  Phase 2: the warp index sits on the top WB row bits,
+    // so both register passes of phase 2 see the same elements per warp and
+    // exchange through a warp barrier.  Phase 1 keeps a CTA barrier: every
+    // row bit is a butterfly bit of one of its passes, so a warp-owned layout
+    // would have to put the lanes on rows and break the coalescing of the
+    // strided phase-1 global accesses.
+    static constexpr int WB = TB - 5;
+    static constexpr bool WARP1 = false;
+    static constexpr bool WARP2 = K2B > 0 && (R1 - CLOG) >= WB;
+    static constexpr uint32_t WM1 = 0u;
+    static constexpr uint32_t WM2 = WARP2 ? (((1u << WB) - 1u) << (MB - WB)) : 0u;
 
     // Pass layouts (forward order).  Phase-1 lambda bits: [S1, MB) (row bits),
     // processed top-down; phase-2 bits [0, R2) (column bits), top-down.
-    using P1A = PassLayout<MB, MB - K1A, K1A, EB>;
-    using P1B = PassLayout<MB, S1, (K1B > 0 ? K1B : 1), EB>;
-    using P2A = PassLayout<MB, R2 - K2A, K2A, EB>;
-    using P2B = PassLayout<MB, 0, (K2B > 0 ? K2B : 1), EB>;
+    using P1A = PassLayout<MB, MB - K1A, K1A, EB, WM1>;
+    using P1B = PassLayout<MB, S1, (K1B > 0 ? K1B : 1), EB, WM1>;
+    using P2A = PassLayout<MB, R2 - K2A, K2A, EB, WM2>;
+    using P2B = PassLayout<MB, 0, (K2B > 0 ? K2B : 1), EB, WM2>;
+
+    // Work-buffer layout (chosen offline; the lane patterns it was chosen
+    // for must be the ones these pass layouts produce).
+    using LT = LayoutTable<LOGN, CLOG, R1, EB, K1A, K2A>;
+    static_assert(LT::lanes_P1A == P1A::kLanes && LT::lanes_P1B == P1B::kLanes &&
+                      LT::lanes_P2A == P2A::kLanes && LT::lanes_P2B == P2B::kLanes,
+                  "layouts_gen.h is stale: rerun gen_layouts.py");
+    using XW = Spread<LT::XW[0], LT::XW[1], LT::XW[2], LT::XW[3]>;
+    static constexpr uint32_t SMEM_WORDS = ((uint32_t)LT::XW[4] + 3u) & ~3u;
+    // dynamic shared memory: work buffer | stage buffer | mbarrier
+    static constexpr uint32_t STAGE_OFF_WORDS = SMEM_WORDS;
+    static constexpr uint32_t MBAR_OFF_WORDS = (STAGE_OFF_WORDS + STAGE_WORDS + 3u) & ~3u;
+    static constexpr uint32_t SMEM_BYTES = (MBAR_OFF_WORDS + 4u) * 4u;  // staged
+    static constexpr uint32_t SMEM_BYTES_DIRECT = SMEM_WORDS * 4u;        // direct
 };
 
-NTT_HD uint32_t smem_phys(uint32_t lam) { return lam + (lam >> 5); }
+// Bulk copy `i` of the input slab of CTA `rank`: word offset in the limb,
+// word offset in the stage buffer, and length in words.  Forward: the
+// phase-1 slab (row rho of the CTA's column range at lambda1 = rho * W1 +
+// kappa'); inverse: the contiguous phase-2 slab [rank*M, (rank+1)*M).  The
+// stage buffer holds lambda at StageLayout::phys(lambda).
+struct SlabCopy {
+    uint32_t src, dst, words;
+};
+template <class G, bool Fwd>
+NTT_HD SlabCopy slab_copy(uint32_t rank, uint32_t i) {
+    if constexpr (Fwd) {
+        constexpr uint32_t per_row = G::W1 / G::COPY_WORDS;
+        const uint32_t row = i / per_row, piece = (i % per_row) * G::COPY_WORDS;
+        return SlabCopy{(row << G::R2) + rank * G::W1 + piece,
+                        StageLayout::phys(row * G::W1 + piece), G::COPY_WORDS};
+    } else {
+        return SlabCopy{rank * G::M + 32u * i, StageLayout::phys(32u * i), 32u};
+    }
+}
+template <class G, bool Fwd>
+NTT_HD constexpr uint32_t slab_copies() {
+    return Fwd ? G::FWD_COPIES : G::INV_COPIES;
+}
 
 // lambda maps (see file header); all linear over disjoint bit sets.
 template <class G>
@@ -143,8 +281,6 @@ struct Maps {
         return ((lam >> G::S1) << G::R2) + (lam & (G::W1 - 1u));
     }
     NTT_HD static uint32_t g1_rank(uint32_t rank) { return rank * G::W1; }
-    // phase-2 slab lambda -> word offset (without rank term rank*M)
-    NTT_HD static uint32_t g2(uint32_t lam) { return lam; }
     // forward scatter: phase-1 lambda -> destination rank / phase-2 lambda
     NTT_HD static uint32_t f_dst(uint32_t lam) { return lam >> (G::MB - G::CLOG); }
     NTT_HD static uint32_t f_lam(uint32_t lam) {
@@ -169,147 +305,182 @@ struct Maps {
 // Register-level stage loops.
 // ---------------------------------------------------------------------------
 
-// Load a block of 2^k consecutive twiddle pairs starting at `idx` (aligned to
-// 2^k) and apply the CT (Fwd) or GS stage that uses them.
-template <class L, class Arith, bool Fwd, int k, class Ctx>
-NTT_HD void stage(Ctx& ctx, uint32_t (&v)[L::E], uint32_t tbase, bool fold_first,
-                  bool fold_last) {
-    // CT: stage k of the pass acts on lambda bit p = PLO + KB - 1 - k, groups
-    // = top k butterfly-coordinate bits.  GS: stage k acts on bit p = PLO + k,
-    // groups = top KB-1-k butterfly bits.
+// Stage k of a pass.  CT (Fwd): acts on lambda bit p = PLO + KB - 1 - k,
+// groups = top k butterfly-coordinate bits.  GS: bit p = PLO + k, groups =
+// top KB-1-k butterfly bits.  `tbase` is the twiddle index of group 0 for
+// this thread; group g of extra-high coordinate xh uses tbase + xoff(xh) + g.
+// Fold: the limb's stage 0 (one twiddle, index 1) with the factor in entry 0.
+template <class L, class Arith, bool Fwd, int k, bool Fold, class Ctx>
+NTT_HD void stage(Ctx& ctx, uint32_t (&v)[L::E], uint32_t tbase) {
     constexpr int p = Fwd ? (L::PLO + L::KB - 1 - k) : (L::PLO + k);
     constexpr int gbits = Fwd ? k : (L::KB - 1 - k);
     constexpr int bbit = Fwd ? (L::KB - 1 - k) : k;  // butterfly coordinate bit
     constexpr int stride = 1 << (bbit + L::XB);      // register distance
-    constexpr int XHB = L::xhi_bits();
+    constexpr int XHB = L::kXHB;
     constexpr int XLB = L::XB - XHB;
     const uint32_t q = ctx.q, q2 = ctx.q2;
-#pragma unroll
-    for (int xh = 0; xh < (1 << XHB); ++xh) {
-        // twiddle slot contribution of the extra bits above the butterfly
-        // range: off >> (p+1) restricted to those bits (a multiple of 2^gbits)
-        uint32_t xoff = L::off(xh << XLB) >> (p + 1);
-#pragma unroll
-        for (int g = 0; g < (1 << gbits); ++g) {
-            TwPair w;
-            if ((Fwd && fold_first) || (!Fwd && fold_last)) {
-                w = ctx.tw(1u);  // stage 0 of the limb: single twiddle index 1
+    if constexpr (Fold) {
+        static_assert(gbits == 0, "stage 0 of the limb has a single group");
+        const TwPair f = ctx.tw_at(0u), w = ctx.tw_at(1u);
+        ct_for<(L::E >> 1)>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            // the E/2 pairs: the lower register has bit (bbit + XB) clear
+            constexpr int r = ((i >> (bbit + L::XB)) << (bbit + L::XB + 1)) | (i & (stride - 1));
+            if constexpr (Fwd) Arith::ct_first(v[r], v[r + stride], f, w, q, q2);
+            else Arith::gs_last(v[r], v[r + stride], f, w, q, q2);
+        });
+    } else {
+        ct_for<(1 << XHB)>([&](auto XH) {
+            constexpr int xh = decltype(XH)::value;
+            constexpr uint32_t xoff = L::off(xh << XLB) >> (p + 1);
+            auto tb = ctx.tw_base(tbase + xoff);
+            // twiddles of this stage for this xh: 2^gbits consecutive pairs
+            TwPair w[1 << gbits];
+            if constexpr (gbits >= 1) {
+                ct_for<(1 << (gbits - 1))>([&](auto G2) {
+                    constexpr int g2 = decltype(G2)::value;
+                    ctx.tw_ld2(tb, 2 * g2, w[2 * g2], w[2 * g2 + 1]);
+                });
             } else {
-                w = ctx.tw(tbase + xoff + (uint32_t)g);
+                w[0] = ctx.tw_ld(tb, 0);
             }
-            // butterflies of group g: bcoord = (g << (bbit+1)) | (lo), lo < 2^bbit
-#pragma unroll
-            for (int lo = 0; lo < (1 << bbit); ++lo) {
-#pragma unroll
-                for (int xl = 0; xl < (1 << XLB); ++xl) {
-                    const int bc = (g << (bbit + 1)) | lo;
-                    const int r = (bc << L::XB) | (xh << XLB) | xl;
-                    if (Fwd) {
-                        if (fold_first)
-                            Arith::ct_first(v[r], v[r + stride], ctx.tw(0u), w, q, q2);
-                        else
-                            Arith::ct(v[r], v[r + stride], w.w, w.wp, q, q2);
-                    } else {
-                        if (fold_last)
-                            Arith::gs_last(v[r], v[r + stride], ctx.tw(0u), w, q, q2);
-                        else
-                            Arith::gs(v[r], v[r + stride], w.w, w.wp, q, q2);
-                    }
-                }
-            }
-        }
+            ct_for<(1 << gbits)>([&](auto Gc) {
+                constexpr int g = decltype(Gc)::value;
+                ct_for<(1 << bbit)>([&](auto LO) {
+                    constexpr int lo = decltype(LO)::value;
+                    ct_for<(1 << XLB)>([&](auto XL) {
+                        constexpr int xl = decltype(XL)::value;
+                        constexpr int bc = (g << (bbit + 1)) | lo;
+                        constexpr int r = (bc << L::XB) | (xh << XLB) | xl;
+                        if constexpr (Fwd) Arith::ct(v[r], v[r + stride], w[g].w, w[g].wp, q, q2);
+                        else Arith::gs(v[r], v[r + stride], w[g].w, w[g].wp, q, q2);
+                    });
+                });
+            });
+        });
     }
 }
 
-// Run all KB stages of a pass.  `phase2` selects the twiddle base rule;
-// `first_is_limb_stage0` / `last_is_limb_stage0`: this pass contains global
-// stage 0 (the forward's first stage / the inverse's last stage), which gets
-// the Montgomery / N^{-1} factor folded in.
-template <class G, class L, class Arith, bool Fwd, bool Phase2, bool HasStage0, class Ctx>
+// Run all KB stages of a pass.  Phase2 selects the twiddle base rule;
+// HasStage0: this pass contains the limb's stage 0 (the forward's first
+// stage / the inverse's last), which gets the Montgomery / N^{-1} fold.
+// ArriveAfterFirst: signal the cluster (relaxed arrive) once stage 0 has
+// consumed every loaded word -- this thread has finished reading its shared
+// memory -- so the wait before the scatter overlaps the remaining stages.
+template <class G, class L, class Arith, bool Fwd, bool Phase2, bool HasStage0,
+          bool ArriveAfterFirst = false, class Ctx>
 NTT_HD void run_stages(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
     using Mp = Maps<G>;
-#define NTTB_STAGE(K)                                                                      \
-    if constexpr ((K) < L::KB) {                                                           \
-        constexpr int p = Fwd ? (L::PLO + L::KB - 1 - (K)) : (L::PLO + (K));               \
-        const uint32_t tb = (Phase2 ? Mp::tw_base_p2(p, ctx.rank) : Mp::tw_base_p1(p)) +   \
-                            (d >> (p + 1));                                                \
-        const bool s0 = HasStage0 && (Fwd ? ((K) == 0) : ((K) == L::KB - 1));             \
-        stage<L, Arith, Fwd, (K)>(ctx, v, tb, Fwd && s0, !Fwd && s0);                      \
-    }
-    NTTB_STAGE(0)
-    NTTB_STAGE(1)
-    NTTB_STAGE(2)
-    NTTB_STAGE(3)
-    NTTB_STAGE(4)
-    NTTB_STAGE(5)
-#undef NTTB_STAGE
+    ct_for<L::KB>([&](auto K) {
+        constexpr int k = decltype(K)::value;
+        constexpr int p = Fwd ? (L::PLO + L::KB - 1 - k) : (L::PLO + k);
+        constexpr bool s0 = HasStage0 && (Fwd ? (k == 0) : (k == L::KB - 1));
+        const uint32_t tb =
+            (Phase2 ? Mp::tw_base_p2(p, ctx.rank) : Mp::tw_base_p1(p)) + (d >> (p + 1));
+        stage<L, Arith, Fwd, k, s0>(ctx, v, tb);
+        if constexpr (ArriveAfterFirst && k == 0) ctx.after_local_reads();
+    });
 }
 
 // ---------------------------------------------------------------------------
-// Loads / stores of a pass's registers.
+// Loads / stores of a pass's registers.  Every address is a per-thread base
+// plus a compile-time constant (an immediate offset on the device).
 // ---------------------------------------------------------------------------
 
-// Vector width (words) usable for a global access whose address map keeps
-// runs of `lim` consecutive lambdas contiguous.
-template <class L>
-constexpr int vec_width(int lim) {
-    int run = 1 << L::run_bits();
-    int w = run < 4 ? run : 4;
-    return w < lim ? w : lim;
+// 16-byte vectors when the thread owns >= 4 consecutive lambdas and the
+// address map keeps runs of `Lim` consecutive lambdas contiguous.
+template <class L, uint32_t Lim>
+constexpr bool use_vec4() {
+    return L::kRunBits >= 2 && Lim >= 4;
 }
 
-template <class L, class Ctx, class AddrFn>
-NTT_HD void load_global(Ctx& ctx, uint32_t (&v)[L::E], uint32_t gbase, AddrFn gmap,
-                        int lim) {
-    // gmap(off) -> global word offset contribution of register offset `off`
-    if (vec_width<L>(lim) == 4 && lim >= 4) {
-#pragma unroll
-        for (int r = 0; r < L::E; ++r) {
-            if ((L::off(r) & 3u) == 0) {
-                uint32_t a, b, c, e;
-                ctx.gload4(gbase + gmap(L::off(r)), a, b, c, e);
-                v[L::reg_of(L::off(r) + 0)] = a;
-                v[L::reg_of(L::off(r) + 1)] = b;
-                v[L::reg_of(L::off(r) + 2)] = c;
-                v[L::reg_of(L::off(r) + 3)] = e;
+// GMap::map(o): word offset of register offset o (linear, no base term)
+template <class L, uint32_t Lim, class GMap, class Ctx>
+NTT_HD void load_global(Ctx& ctx, uint32_t (&v)[L::E], uint32_t gbase) {
+    auto gb = ctx.g_base(gbase);
+    if constexpr (use_vec4<L, Lim>()) {
+        ct_for<L::E>([&](auto R) {
+            constexpr int r = decltype(R)::value;
+            constexpr uint32_t o = L::off(r);
+            if constexpr ((o & 3u) == 0) {
+                ctx.g_ld4(gb, GMap::map(o), v[L::reg_of(o)], v[L::reg_of(o + 1)],
+                          v[L::reg_of(o + 2)], v[L::reg_of(o + 3)]);
             }
-        }
+        });
     } else {
-#pragma unroll
-        for (int r = 0; r < L::E; ++r) v[r] = ctx.gload(gbase + gmap(L::off(r)));
+        ct_for<L::E>([&](auto R) {
+            constexpr int r = decltype(R)::value;
+            v[r] = ctx.g_ld(gb, GMap::map(L::off(r)));
+        });
     }
 }
 
-template <class L, class Ctx, class AddrFn, class ValFn>
-NTT_HD void store_global(Ctx& ctx, uint32_t (&v)[L::E], uint32_t gbase, AddrFn gmap,
-                         int lim, ValFn fin) {
-    if (vec_width<L>(lim) == 4 && lim >= 4) {
-#pragma unroll
-        for (int r = 0; r < L::E; ++r) {
-            if ((L::off(r) & 3u) == 0) {
-                ctx.gstore4(gbase + gmap(L::off(r)), fin(v[L::reg_of(L::off(r) + 0)]),
-                            fin(v[L::reg_of(L::off(r) + 1)]), fin(v[L::reg_of(L::off(r) + 2)]),
-                            fin(v[L::reg_of(L::off(r) + 3)]));
+template <class L, uint32_t Lim, class GMap, class Ctx, class ValFn>
+NTT_HD void store_global(Ctx& ctx, uint32_t (&v)[L::E], uint32_t gbase, ValFn fin) {
+    auto gb = ctx.g_base(gbase);
+    if constexpr (use_vec4<L, Lim>()) {
+        ct_for<L::E>([&](auto R) {
+            constexpr int r = decltype(R)::value;
+            constexpr uint32_t o = L::off(r);
+            if constexpr ((o & 3u) == 0) {
+                ctx.g_st4(gb, GMap::map(o), fin(v[L::reg_of(o)]), fin(v[L::reg_of(o + 1)]),
+                          fin(v[L::reg_of(o + 2)]), fin(v[L::reg_of(o + 3)]));
             }
-        }
+        });
     } else {
-#pragma unroll
-        for (int r = 0; r < L::E; ++r) ctx.gstore(gbase + gmap(L::off(r)), fin(v[r]));
+        ct_for<L::E>([&](auto R) {
+            constexpr int r = decltype(R)::value;
+            ctx.g_st(gb, GMap::map(L::off(r)), fin(v[r]));
+        });
     }
 }
 
+// Stage buffer (the bulk-copied input slab).
 template <class L, class Ctx>
+NTT_HD void load_stage(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
+    auto sb = ctx.st_base(StageLayout::phys(d));
+    if constexpr (L::kRunBits >= 2) {
+        ct_for<L::E>([&](auto R) {
+            constexpr int r = decltype(R)::value;
+            constexpr uint32_t o = L::off(r);
+            if constexpr ((o & 3u) == 0)
+                ctx.st_ld4(sb, StageLayout::phys(o), v[L::reg_of(o)], v[L::reg_of(o + 1)],
+                           v[L::reg_of(o + 2)], v[L::reg_of(o + 3)]);
+        });
+    } else {
+        ct_for<L::E>([&](auto R) {
+            constexpr int r = decltype(R)::value;
+            v[r] = ctx.st_ld(sb, StageLayout::phys(L::off(r)));
+        });
+    }
+}
+
+// The input slab of a transform: from the stage buffer (bulk-copied ahead of
+// time) or straight from global memory, as the context's kStaged says.
+template <class L, uint32_t Lim, class GMap, class Ctx>
+NTT_HD void load_input(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d, uint32_t gbase) {
+    if constexpr (Ctx::kStaged)
+        load_stage<L>(ctx, v, d);
+    else
+        load_global<L, Lim, GMap>(ctx, v, gbase);
+}
+
+template <class L, class X, class Ctx>
 NTT_HD void load_smem(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
-    const uint32_t base = smem_phys(d);
-#pragma unroll
-    for (int r = 0; r < L::E; ++r) v[r] = ctx.sload(base + smem_phys(L::off(r)));
+    auto sb = ctx.s_base(X::phys(d));
+    ct_for<L::E>([&](auto R) {
+        constexpr int r = decltype(R)::value;
+        v[r] = ctx.s_ld(sb, X::phys(L::off(r)));
+    });
 }
 
-template <class L, class Ctx>
+template <class L, class X, class Ctx>
 NTT_HD void store_smem(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
-    const uint32_t base = smem_phys(d);
-#pragma unroll
-    for (int r = 0; r < L::E; ++r) ctx.sstore(base + smem_phys(L::off(r)), v[r]);
+    auto sb = ctx.s_base(X::phys(d));
+    ct_for<L::E>([&](auto R) {
+        constexpr int r = decltype(R)::value;
+        ctx.s_st(sb, X::phys(L::off(r)), v[r]);
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -327,148 +498,170 @@ struct FwdFinal {
     NTT_HD uint32_t operator()(uint32_t x) const { return Arith::fwd_final(x, q, q2); }
 };
 
+// Global-offset maps of the two slab layouts (register-offset part).
+template <class G>
+struct G1Map {
+    static constexpr uint32_t map(uint32_t o) {
+        return ((o >> G::S1) << G::R2) + (o & (G::W1 - 1u));
+    }
+};
+struct G2Map {
+    static constexpr uint32_t map(uint32_t o) { return o; }
+};
+
+// Scatter maps (register-offset part), see Maps.
+template <class G>
+struct FDst {
+    static constexpr uint32_t map(uint32_t o) { return o >> (G::MB - G::CLOG); }
+};
+template <class G>
+struct FLam {
+    static constexpr uint32_t map(uint32_t o) {
+        return (((o >> G::S1) & (G::H2 - 1u)) << G::R2) + (o & (G::W1 - 1u));
+    }
+};
+template <class G>
+struct IDst {
+    static constexpr uint32_t map(uint32_t o) { return (o & ((1u << G::R2) - 1u)) >> G::S1; }
+};
+template <class G>
+struct ILam {
+    static constexpr uint32_t map(uint32_t o) {
+        return ((o >> G::R2) << G::S1) + (o & (G::W1 - 1u));
+    }
+};
+
+// Scatter one pass's registers to their owners' shared memory (DSMEM when
+// C > 1).  The destination word is phys(base) + phys(map(offset)).
+template <class L, class X, class Ctx, class DstF, class LamF>
+NTT_HD void scatter_regs(Ctx& ctx, uint32_t (&v)[L::E], uint32_t dd, uint32_t dl) {
+    ct_for<L::E>([&](auto R) {
+        constexpr int r = decltype(R)::value;
+        constexpr uint32_t o = L::off(r);
+        auto rb = ctx.r_base(dd + DstF::map(o), X::phys(dl));
+        ctx.template r_st<X::phys(LamF::map(o))>(rb, v[r]);
+    });
+}
+
 template <class G, class Arith, class Ctx>
 struct Forward {
     using Mp = Maps<G>;
+    using X = typename G::XW;
     using P1A = typename G::P1A;
     using P1B = typename G::P1B;
     using P2A = typename G::P2A;
     using P2B = typename G::P2B;
 
-    struct G1 {
-        NTT_HD uint32_t operator()(uint32_t o) const { return Maps<G>::g1(o); }
-    };
-    struct G2 {
-        NTT_HD uint32_t operator()(uint32_t o) const { return o; }
-    };
-
-    // Scatter a phase-1 pass's registers to the phase-2 owners.
     template <class L>
     NTT_HD static void scatter(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
-        const uint32_t dd = Mp::f_dst(d);
-        const uint32_t dl = Mp::f_lam(d) + Mp::g1_rank(ctx.rank);
-#pragma unroll
-        for (int r = 0; r < L::E; ++r) {
-            const uint32_t o = L::off(r);
-            ctx.rstore(dd + Mp::f_dst(o), smem_phys(dl + Mp::f_lam(o)), v[r]);
-        }
+        scatter_regs<L, X, Ctx, FDst<G>, FLam<G>>(ctx, v, Mp::f_dst(d),
+                                                 Mp::f_lam(d) + Mp::g1_rank(ctx.rank));
     }
 
-    // Phase-1 first pass: global (normal domain) -> stages incl. stage 0 ->
-    // SMEM (if a second phase-1 pass follows) or the scatter.
+    // Phase-1 first pass: input slab (normal domain) -> stages incl. stage 0
+    // -> work buffer (if a second phase-1 pass follows) or the scatter.
     NTT_HD static void pass1a(Ctx& ctx, uint32_t tid) {
         uint32_t v[P1A::E];
         const uint32_t d = P1A::dep(tid);
-        load_global<P1A>(ctx, v, Mp::g1(d) + Mp::g1_rank(ctx.rank), G1{}, (int)G::W1);
-        run_stages<G, P1A, Arith, true, false, true>(ctx, v, d);
+        load_input<P1A, G::W1, G1Map<G>>(ctx, v, d, Mp::g1(d) + Mp::g1_rank(ctx.rank));
+        run_stages<G, P1A, Arith, true, false, true, (G::K1B == 0)>(ctx, v, d);
         if constexpr (G::K1B > 0) {
-            store_smem<P1A>(ctx, v, d);
+            store_smem<P1A, X>(ctx, v, d);
         } else {
-            ctx.after_local_reads();
             ctx.before_scatter();
             scatter<P1A>(ctx, v, d);
         }
     }
     NTT_HD static void pass1b(Ctx& ctx, uint32_t tid) {
-        uint32_t v[P1B::E];
-        const uint32_t d = P1B::dep(tid);
-        load_smem<P1B>(ctx, v, d);
-        ctx.after_local_reads();
-        run_stages<G, P1B, Arith, true, false, false>(ctx, v, d);
-        ctx.before_scatter();
-        scatter<P1B>(ctx, v, d);
+        if constexpr (G::K1B > 0) {
+            uint32_t v[P1B::E];
+            const uint32_t d = P1B::dep(tid);
+            load_smem<P1B, X>(ctx, v, d);
+            run_stages<G, P1B, Arith, true, false, false, true>(ctx, v, d);
+            ctx.before_scatter();
+            scatter<P1B>(ctx, v, d);
+        }
     }
     NTT_HD static void pass2a(Ctx& ctx, uint32_t tid) {
         uint32_t v[P2A::E];
         const uint32_t d = P2A::dep(tid);
-        load_smem<P2A>(ctx, v, d);
+        load_smem<P2A, X>(ctx, v, d);
         run_stages<G, P2A, Arith, true, true, false>(ctx, v, d);
         if constexpr (G::K2B > 0) {
-            store_smem<P2A>(ctx, v, d);
+            store_smem<P2A, X>(ctx, v, d);
         } else {
-            store_global<P2A>(ctx, v, d + ctx.rank * G::M, G2{}, 1 << 30,
-                              FwdFinal<Arith>{ctx.q, ctx.q2});
+            store_global<P2A, (1u << 30), G2Map>(ctx, v, d + ctx.rank * G::M,
+                                                 FwdFinal<Arith>{ctx.q, ctx.q2});
         }
     }
     NTT_HD static void pass2b(Ctx& ctx, uint32_t tid) {
-        uint32_t v[P2B::E];
-        const uint32_t d = P2B::dep(tid);
-        load_smem<P2B>(ctx, v, d);
-        run_stages<G, P2B, Arith, true, true, false>(ctx, v, d);
-        store_global<P2B>(ctx, v, d + ctx.rank * G::M, G2{}, 1 << 30,
-                          FwdFinal<Arith>{ctx.q, ctx.q2});
+        if constexpr (G::K2B > 0) {
+            uint32_t v[P2B::E];
+            const uint32_t d = P2B::dep(tid);
+            load_smem<P2B, X>(ctx, v, d);
+            run_stages<G, P2B, Arith, true, true, false>(ctx, v, d);
+            store_global<P2B, (1u << 30), G2Map>(ctx, v, d + ctx.rank * G::M,
+                                                 FwdFinal<Arith>{ctx.q, ctx.q2});
+        }
     }
 };
 
 template <class G, class Arith, class Ctx>
 struct Inverse {
     using Mp = Maps<G>;
+    using X = typename G::XW;
     using P1A = typename G::P1A;
     using P1B = typename G::P1B;
     using P2A = typename G::P2A;
     using P2B = typename G::P2B;
 
-    struct G1 {
-        NTT_HD uint32_t operator()(uint32_t o) const { return Maps<G>::g1(o); }
-    };
-    struct G2 {
-        NTT_HD uint32_t operator()(uint32_t o) const { return o; }
-    };
-
     template <class L>
     NTT_HD static void scatter(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
-        const uint32_t dd = Mp::i_dst(d);
-        const uint32_t dl = Mp::i_lam(d) + Mp::i_lam_rank(ctx.rank);
-#pragma unroll
-        for (int r = 0; r < L::E; ++r) {
-            const uint32_t o = L::off(r);
-            ctx.rstore(dd + Mp::i_dst(o), smem_phys(dl + Mp::i_lam(o)), v[r]);
-        }
+        scatter_regs<L, X, Ctx, IDst<G>, ILam<G>>(ctx, v, Mp::i_dst(d),
+                                                 Mp::i_lam(d) + Mp::i_lam_rank(ctx.rank));
     }
 
     // Inverse order of passes: P2B (low column bits), P2A, scatter, P1B, P1A.
-    // The first pass reads the contiguous phase-2 slab from global.
-    template <class L, bool Last>
-    NTT_HD static void phase2_pass(Ctx& ctx, uint32_t tid, bool from_global) {
+    // The first pass reads the contiguous phase-2 slab (stage or global).
+    template <class L, bool Last, bool FromInput>
+    NTT_HD static void phase2_pass(Ctx& ctx, uint32_t tid) {
         uint32_t v[L::E];
         const uint32_t d = L::dep(tid);
-        if (from_global)
-            load_global<L>(ctx, v, d + ctx.rank * G::M, G2{}, 1 << 30);
+        if constexpr (FromInput)
+            load_input<L, (1u << 30), G2Map>(ctx, v, d, d + ctx.rank * G::M);
         else
-            load_smem<L>(ctx, v, d);
-        if (Last) ctx.after_local_reads();
-        run_stages<G, L, Arith, false, true, false>(ctx, v, d);
-        if (Last) {
+            load_smem<L, X>(ctx, v, d);
+        run_stages<G, L, Arith, false, true, false, Last>(ctx, v, d);
+        if constexpr (Last) {
             ctx.before_scatter();
             scatter<L>(ctx, v, d);
         } else {
-            store_smem<L>(ctx, v, d);
+            store_smem<L, X>(ctx, v, d);
         }
     }
     NTT_HD static void pass2b(Ctx& ctx, uint32_t tid) {
-        if constexpr (G::K2B > 0) phase2_pass<P2B, false>(ctx, tid, true);
+        if constexpr (G::K2B > 0) phase2_pass<P2B, false, true>(ctx, tid);
     }
     NTT_HD static void pass2a(Ctx& ctx, uint32_t tid) {
-        phase2_pass<P2A, true>(ctx, tid, G::K2B == 0);
+        phase2_pass<P2A, true, G::K2B == 0>(ctx, tid);
     }
     NTT_HD static void pass1b(Ctx& ctx, uint32_t tid) {
         if constexpr (G::K1B > 0) {
             uint32_t v[P1B::E];
             const uint32_t d = P1B::dep(tid);
-            load_smem<P1B>(ctx, v, d);
+            load_smem<P1B, X>(ctx, v, d);
             run_stages<G, P1B, Arith, false, false, false>(ctx, v, d);
-            store_smem<P1B>(ctx, v, d);
+            store_smem<P1B, X>(ctx, v, d);
         }
     }
-    // Last pass: contains global stage 0 (fold N^{-1} R^{-1}), canonical
+    // Last pass: contains the limb's stage 0 (fold N^{-1} R^{-1}), canonical
     // output to the phase-1 slab in global memory.
     NTT_HD static void pass1a(Ctx& ctx, uint32_t tid) {
         uint32_t v[P1A::E];
         const uint32_t d = P1A::dep(tid);
-        load_smem<P1A>(ctx, v, d);
+        load_smem<P1A, X>(ctx, v, d);
         run_stages<G, P1A, Arith, false, false, true>(ctx, v, d);
-        store_global<P1A>(ctx, v, Mp::g1(d) + Mp::g1_rank(ctx.rank), G1{}, (int)G::W1,
-                          Ident{});
+        store_global<P1A, G::W1, G1Map<G>>(ctx, v, Mp::g1(d) + Mp::g1_rank(ctx.rank), Ident{});
     }
 };
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include "../../include/ntt_b200.h"
+#include "../../include/ntt_b200_tune.h"
 #include "configs.h"
 #include "fused_kernel.cuh"
 
@@ -11,17 +12,23 @@ namespace nttb {
 ntt_status_t fail(ntt_status_t st, const char* fmt, ...);
 ntt_status_t cuda_fail(cudaError_t e, const char* what);
 
-const FusedConfig* default_config(int logN);
+// Untuned default for (logN, direction); config_by_r1 matches a phase split.
+const FusedConfig* default_config(int logN, bool fwd = true);
 const FusedConfig* config_by_r1(int logN, int r1);
 const FusedConfig* config_by_index(int idx);
-// Autotuned choice for (logN, limbs) on the current device, or nullptr.
-const FusedConfig* tuned_config(int logN, int limbs);
-ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s);
+// Autotuned choice for (logN, limbs, direction) on the current device, or
+// nullptr.
+const FusedConfig* tuned_config(int logN, int limbs, bool fwd);
+// Clusters of this configuration resident at once on the current device.
+int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule);
+// One launch of a fused configuration under a schedule (NTT_SCHEDULE_*).
+ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
+                          int schedule);
 ntt_status_t validate_modulus(int logN, ModulusConfig m, ModulusRuntime* rt);
 // One launch over `polys` polynomials of `limbs` limbs (cfg == nullptr: the
-// single-CTA small-size kernel).
+// single-CTA small-size kernel).  status: optional device error word.
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
-                           cudaStream_t s);
+                           cudaStream_t s, uint32_t* status, int schedule);
 
 }  // namespace nttb

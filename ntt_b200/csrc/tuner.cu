@@ -1,11 +1,13 @@
-// Autotuner: sweep the compiled configurations for (logN, limbs), time them
-// on the device, keep the fastest (in memory and in an on-disk cache).
+// Autotuner: sweep the compiled configurations for (logN, limbs), time the
+// forward and the inverse launch of each on the device, keep the fastest per
+// direction (in memory and in an on-disk cache).
 //
 // Replaces the reference's compile-time choice of phase triples
 // (DefaultNTTLaunchConfig<LogN>, src/ntt_config.h:62-73): the triple is now
-// picked per (logN, limb count) at run time, "sweep, then cache".
+// picked per (logN, limb count, direction) at run time, "sweep, then cache".
 // Cache file: $NTT_B200_TUNE_CACHE, else $HOME/.cache/ntt_b200/tune.txt;
-// one line per entry: "<device-name>|<sm-count> <logN> <limb-bucket> <config-index> <us>".
+// one line per entry:
+//   "<device-name>|<sm-count> <logN> <limb-bucket> <fwd|inv> <config-index> <us>".
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -18,7 +20,6 @@
 #include <tuple>
 #include <vector>
 
-#include "../../include/ntt_b200_tune.h"
 #include "runtime.h"
 
 using namespace nttb;
@@ -27,8 +28,8 @@ namespace {
 
 std::mutex g_mu;
 bool g_loaded = false;
-// key: device id string, logN, limb bucket -> config index
-std::map<std::tuple<std::string, int, int>, std::pair<int, double>> g_table;
+// key: device id, logN, limb bucket, direction (1 = forward)
+std::map<std::tuple<std::string, int, int, int>, std::pair<int, double>> g_table;
 
 int limb_bucket(int limbs) {  // 1, 2-4, 5-16, 17-64, 65+
     if (limbs <= 1) return 0;
@@ -60,12 +61,13 @@ void load_locked() {
     g_loaded = true;
     FILE* f = fopen(cache_path().c_str(), "r");
     if (!f) return;
-    char dev[256];
+    char dev[256], dir[8];
     int logN, bucket, idx;
     double us;
-    while (fscanf(f, "%255s %d %d %d %lf", dev, &logN, &bucket, &idx, &us) == 5) {
+    while (fscanf(f, "%255s %d %d %7s %d %lf", dev, &logN, &bucket, dir, &idx, &us) == 6) {
         const FusedConfig* c = config_by_index(idx);
-        if (c && c->logN == logN) g_table[{dev, logN, bucket}] = {idx, us};
+        if (c && c->logN == logN)
+            g_table[{dev, logN, bucket, std::string(dir) == "fwd" ? 1 : 0}] = {idx, us};
     }
     fclose(f);
 }
@@ -73,34 +75,36 @@ void load_locked() {
 void save_locked() {
     std::string path = cache_path();
     std::string dir = path.substr(0, path.find_last_of('/'));
-    // create parent directories (best effort)
-    for (size_t i = 1; i <= dir.size(); ++i)
+    for (size_t i = 1; i <= dir.size(); ++i)  // parent directories, best effort
         if (i == dir.size() || dir[i] == '/') mkdir(dir.substr(0, i).c_str(), 0755);
     FILE* f = fopen(path.c_str(), "w");
     if (!f) return;
     for (auto& kv : g_table)
-        fprintf(f, "%s %d %d %d %.3f\n", std::get<0>(kv.first).c_str(), std::get<1>(kv.first),
-                std::get<2>(kv.first), kv.second.first, kv.second.second);
+        fprintf(f, "%s %d %d %s %d %.3f\n", std::get<0>(kv.first).c_str(), std::get<1>(kv.first),
+                std::get<2>(kv.first), std::get<3>(kv.first) ? "fwd" : "inv", kv.second.first,
+                kv.second.second);
     fclose(f);
 }
 
+// Deterministic filler below every supported modulus (the timed transforms
+// do not depend on the values).
 __global__ void fill_kernel(uint32_t* a, size_t n, uint32_t seed) {
     size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i < n) {
         uint32_t x = (uint32_t)i * 2654435761u ^ seed;
         x ^= x >> 13;
         x *= 0x5bd1e995u;
-        a[i] = (x ^ (x >> 15)) & 0x1fffffffu;  // below every supported modulus
+        a[i] = (x ^ (x >> 15)) & 0x1fffffffu;
     }
 }
 
 }  // namespace
 
 namespace nttb {
-const FusedConfig* tuned_config(int logN, int limbs) {
+const FusedConfig* tuned_config(int logN, int limbs, bool fwd) {
     std::lock_guard<std::mutex> lk(g_mu);
     load_locked();
-    auto it = g_table.find({device_key(), logN, limb_bucket(limbs)});
+    auto it = g_table.find({device_key(), logN, limb_bucket(limbs), fwd ? 1 : 0});
     if (it == g_table.end()) return nullptr;
     return config_by_index(it->second.first);
 }
@@ -113,9 +117,15 @@ int ntt_config_count(void) { return fused_config_count(); }
 ntt_status_t ntt_config_get(int index, ntt_kernel_config_t* out) {
     const FusedConfig* c = config_by_index(index);
     if (!c || !out) return fail(NTT_ERR_INVALID_ARGUMENT, "bad config index %d", index);
-    *out = ntt_kernel_config_t{c->logN, 1 << c->clog, c->r1, c->eb, c->k1a, c->k2a, c->threads,
-                               c->smem_bytes};
+    *out = ntt_kernel_config_t{c->logN, 1 << c->clog, c->r1,     c->eb,
+                               c->k1a,  c->k2a,       c->threads, c->smem_bytes_direct};
     return NTT_OK;
+}
+
+int ntt_config_resident_clusters(int index, int forward, int schedule) {
+    const FusedConfig* c = config_by_index(index);
+    if (!c) return -1;
+    return config_resident_clusters(c, forward != 0, schedule);
 }
 
 ntt_status_t ntt_autotune(int logN, int limbs, int polys, int iters, ntt_tune_result_t* out) {
@@ -134,10 +144,10 @@ ntt_status_t ntt_autotune(int logN, int limbs, int polys, int iters, ntt_tune_re
     const size_t words = (size_t)polys * limbs << logN;
     uint32_t* data = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    ntt_status_t st = NTT_OK;
     cudaStream_t s = nullptr;
-    double best = 1e30;
-    int best_idx = -1;
+    ntt_status_t st = NTT_OK;
+    double best[2] = {1e30, 1e30};
+    int best_idx[2] = {-1, -1};
     cudaError_t ce = cudaMalloc(&data, words * 4);
     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
@@ -147,27 +157,26 @@ ntt_status_t ntt_autotune(int logN, int limbs, int polys, int iters, ntt_tune_re
         fill_kernel<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(data, words, 1234u);
         for (int idx : cand) {
             const FusedConfig* c = config_by_index(idx);
-            float ms = 0;
-            for (int rep = 0; rep < 2 && st == NTT_OK; ++rep) {  // rep 0 = warm-up
-                cudaEventRecord(e0, s);
-                for (int it = 0; it < iters && st == NTT_OK; ++it) {
-                    st = run_transform(logN, c, (const TwPair*)tw_f, qd, limbs, data, polys,
-                                       (size_t)limbs << logN, true, s);
-                    if (st == NTT_OK)
-                        st = run_transform(logN, c, (const TwPair*)tw_i, qd, limbs, data, polys,
-                                           (size_t)limbs << logN, false, s);
+            for (int dir = 1; dir >= 0 && st == NTT_OK; --dir) {  // 1 = forward
+                float ms = 0;
+                for (int rep = 0; rep < 2 && st == NTT_OK; ++rep) {  // rep 0 = warm-up
+                    cudaEventRecord(e0, s);
+                    for (int it = 0; it < iters && st == NTT_OK; ++it)
+                        st = run_transform(logN, c, (const TwPair*)(dir ? tw_f : tw_i), qd, limbs,
+                                           data, polys, (size_t)limbs << logN, dir == 1, s,
+                                           nullptr, NTT_SCHEDULE_DIRECT);
+                    cudaEventRecord(e1, s);
+                    ce = cudaEventSynchronize(e1);
+                    if (ce != cudaSuccess) st = cuda_fail(ce, "autotune timing");
+                    cudaEventElapsedTime(&ms, e0, e1);
                 }
-                cudaEventRecord(e1, s);
-                ce = cudaEventSynchronize(e1);
-                if (ce != cudaSuccess) st = cuda_fail(ce, "autotune timing");
-                cudaEventElapsedTime(&ms, e0, e1);
+                const double us = 1000.0 * ms / iters;
+                if (st == NTT_OK && us < best[dir]) {
+                    best[dir] = us;
+                    best_idx[dir] = idx;
+                }
             }
             if (st != NTT_OK) break;
-            const double us = 1000.0 * ms / iters;
-            if (us < best) {
-                best = us;
-                best_idx = idx;
-            }
         }
     }
     if (e0) cudaEventDestroy(e0);
@@ -179,12 +188,15 @@ ntt_status_t ntt_autotune(int logN, int limbs, int polys, int iters, ntt_tune_re
     {
         std::lock_guard<std::mutex> lk(g_mu);
         load_locked();
-        g_table[{device_key(), logN, limb_bucket(limbs)}] = {best_idx, best};
+        g_table[{device_key(), logN, limb_bucket(limbs), 1}] = {best_idx[1], best[1]};
+        g_table[{device_key(), logN, limb_bucket(limbs), 0}] = {best_idx[0], best[0]};
         save_locked();
     }
     if (out) {
-        out->config_index = best_idx;
-        out->roundtrip_us = best;
+        out->fwd_index = best_idx[1];
+        out->inv_index = best_idx[0];
+        out->fwd_us = best[1];
+        out->inv_us = best[0];
         out->candidates = (int)cand.size();
     }
     return NTT_OK;

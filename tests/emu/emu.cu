@@ -2,17 +2,21 @@
 //
 // Runs the very same pass functions as the device kernels (ntt_core.cuh) on
 // the host, thread by thread, with the barriers between passes implied, and
-// checks what a GPU run cannot show safely: every global / shared / DSMEM
-// access is in bounds, every scatter and store covers its destination
-// exactly once, and how many ways each warp-wide shared-memory access is
-// bank-conflicted.  Built by tests/emu/Makefile into libntt_emu.so (host
-// code only; nothing here runs on a GPU).
+// checks what a GPU run cannot show safely: every global / stage / shared /
+// DSMEM access is in bounds, the bulk copies cover the stage buffer and every
+// scatter and store covers its destination exactly once, every read after a
+// warp barrier reads words its own warp wrote, and how many ways each
+// warp-wide shared-memory access is bank-conflicted.  Built by
+// tests/emu/Makefile into libntt_emu.so (host code only; nothing here runs on
+// a GPU).
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
-#include <stdexcept>
 #include <string>
+#include <tuple>
+#include <utility>
 #include <vector>
 
 #include "../../ntt_b200/csrc/configs.h"
@@ -23,25 +27,31 @@ using namespace nttb;
 namespace {
 
 struct Access {
-    uint32_t warp, seq, kind, rank_dst;
+    uint32_t warp, seq, kind, rank_dst;  // kind: 0 lds, 1 sts, 2 dsmem, 3 stage128
     uint32_t addr;
+    uint32_t src;  // issuing CTA
 };
 
 struct EmuCluster {
     int C = 1;
     uint32_t smem_words = 0;
     std::vector<std::vector<uint32_t>> smem;
-    // DSMEM scatter target: the device orders every CTA's local reads of a
-    // step before any remote store lands (cluster arrive/wait), so remote
-    // stores go to a shadow copy that is committed when the step ends.
+    // Scatter target: the device orders every CTA's local reads of a step
+    // before any remote store lands (cluster arrive/wait), so scattered words
+    // go to a shadow copy committed when the step ends.
     std::vector<std::vector<uint32_t>> shadow;
-    std::vector<std::vector<uint32_t>> writes;  // per word write count in current step
-    std::vector<std::vector<uint32_t>> rwrites;
+    std::vector<std::vector<uint32_t>> writes;   // per-word write count, this step
+    std::vector<std::vector<uint32_t>> rwrites;  // scattered words, this step
+    std::vector<std::vector<uint32_t>> writer;   // warp that last wrote each word
+    std::vector<std::vector<uint32_t>> stage;    // padded input slab per CTA
+    bool warp_local = false;                     // this step follows a warp barrier
     std::vector<Access> log;
     std::string err;
 };
 
+template <bool Staged>
 struct EmuCtx {
+    static constexpr bool kStaged = Staged;
     EmuCluster* cl;
     uint32_t* g;
     uint32_t glen;
@@ -53,73 +63,162 @@ struct EmuCtx {
 
     void fail(const char* what, uint64_t v) {
         if (cl->err.empty()) {
-            char b[160];
-            snprintf(b, sizeof b, "%s out of range: %llu (rank %u tid %u)", what,
-                     (unsigned long long)v, rank, tid);
+            char b[200];
+            snprintf(b, sizeof b, "%s: %llu (rank %u tid %u)", what, (unsigned long long)v, rank,
+                     tid);
             cl->err = b;
         }
     }
-    uint32_t gload(uint32_t o) {
-        if (o >= glen) { fail("gload", o); return 0; }
+    // global: base and offsets are word indices into the limb
+    uint32_t g_base(uint32_t o) { return o; }
+    uint32_t g_ld(uint32_t b, uint32_t c) {
+        const uint32_t o = b + c;
+        if (o >= glen) {
+            fail("g_ld out of range", o);
+            return 0;
+        }
         return g[o];
     }
-    void gload4(uint32_t o, uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d) {
-        if (o % 4 || o + 3 >= glen) { fail("gload4", o); a = b = c = d = 0; return; }
-        a = g[o]; b = g[o + 1]; c = g[o + 2]; d = g[o + 3];
+    void g_ld4(uint32_t b, uint32_t c, uint32_t& x, uint32_t& y, uint32_t& z, uint32_t& w) {
+        const uint32_t o = b + c;
+        if (o % 4 || o + 3 >= glen) {
+            fail("g_ld4 out of range or misaligned", o);
+            x = y = z = w = 0;
+            return;
+        }
+        x = g[o];
+        y = g[o + 1];
+        z = g[o + 2];
+        w = g[o + 3];
     }
-    void gstore(uint32_t o, uint32_t v) {
-        if (o >= glen) { fail("gstore", o); return; }
+    void g_st(uint32_t b, uint32_t c, uint32_t v) {
+        const uint32_t o = b + c;
+        if (o >= glen) {
+            fail("g_st out of range", o);
+            return;
+        }
         g[o] = v;
         (*gwrites)[o]++;
     }
-    void gstore4(uint32_t o, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-        if (o % 4 || o + 3 >= glen) { fail("gstore4", o); return; }
-        g[o] = a; g[o + 1] = b; g[o + 2] = c; g[o + 3] = d;
+    void g_st4(uint32_t b, uint32_t c, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+        const uint32_t o = b + c;
+        if (o % 4 || o + 3 >= glen) {
+            fail("g_st4 out of range or misaligned", o);
+            return;
+        }
+        g[o] = x;
+        g[o + 1] = y;
+        g[o + 2] = z;
+        g[o + 3] = w;
         for (int i = 0; i < 4; ++i) (*gwrites)[o + i]++;
     }
-    uint32_t sload(uint32_t w) {
-        if (w >= cl->smem_words) { fail("sload", w); return 0; }
-        cl->log.push_back({tid / 32, seq++, 0, rank, w});
+    // stage buffer
+    uint32_t st_base(uint32_t w) { return w; }
+    uint32_t st_ld(uint32_t b, uint32_t c) {
+        const uint32_t w = b + c;
+        if (w >= cl->stage[rank].size()) {
+            fail("st_ld out of range", w);
+            return 0;
+        }
+        cl->log.push_back({tid / 32, seq++, 0, rank, w, rank});
+        return cl->stage[rank][w];
+    }
+    void st_ld4(uint32_t b, uint32_t c, uint32_t& x, uint32_t& y, uint32_t& z, uint32_t& w4) {
+        const uint32_t w = b + c;
+        if (w % 4 || w + 3 >= cl->stage[rank].size()) {
+            fail("st_ld4 out of range or misaligned", w);
+            x = y = z = w4 = 0;
+            return;
+        }
+        cl->log.push_back({tid / 32, seq++, 3, (tid % 32) / 8, w, rank});
+        x = cl->stage[rank][w];
+        y = cl->stage[rank][w + 1];
+        z = cl->stage[rank][w + 2];
+        w4 = cl->stage[rank][w + 3];
+    }
+    // work buffer
+    uint32_t s_base(uint32_t w) { return w; }
+    uint32_t s_ld(uint32_t b, uint32_t c) {
+        const uint32_t w = b + c;
+        if (w >= cl->smem_words) {
+            fail("s_ld out of range", w);
+            return 0;
+        }
+        cl->log.push_back({tid / 32, seq++, 0, rank, w, rank});
+        if (cl->warp_local && cl->writer[rank][w] != tid / 32)
+            fail("warp-local read of another warp's word", w);
         return cl->smem[rank][w];
     }
-    void sstore(uint32_t w, uint32_t v) {
-        if (w >= cl->smem_words) { fail("sstore", w); return; }
-        cl->log.push_back({tid / 32, seq++, 1, rank, w});
+    void s_st(uint32_t b, uint32_t c, uint32_t v) {
+        const uint32_t w = b + c;
+        if (w >= cl->smem_words) {
+            fail("s_st out of range", w);
+            return;
+        }
+        cl->log.push_back({tid / 32, seq++, 1, rank, w, rank});
         cl->smem[rank][w] = v;
+        cl->writer[rank][w] = tid / 32;
         cl->writes[rank][w]++;
     }
-    void rstore(uint32_t dst, uint32_t w, uint32_t v) {
-        if (dst >= (uint32_t)cl->C) { fail("rstore rank", dst); return; }
-        if (w >= cl->smem_words) { fail("rstore", w); return; }
-        cl->log.push_back({tid / 32, seq++, 2, dst, w});
+    std::pair<uint32_t, uint32_t> r_base(uint32_t dst, uint32_t w) { return {dst, w}; }
+    template <uint32_t Off>
+    void r_st(std::pair<uint32_t, uint32_t> rb, uint32_t v) {
+        const uint32_t dst = rb.first, w = rb.second + Off;
+        if (dst >= (uint32_t)cl->C) {
+            fail("r_st rank out of range", dst);
+            return;
+        }
+        if (w >= cl->smem_words) {
+            fail("r_st out of range", w);
+            return;
+        }
+        cl->log.push_back({tid / 32, seq++, 2, dst, w, rank});
         cl->shadow[dst][w] = v;
         cl->writes[dst][w]++;
         cl->rwrites[dst][w]++;
     }
-    TwPair tw(uint32_t i) {
-        if (i >= twlen) { fail("twiddle", i); return TwPair{0, 0}; }
+    TwPair tw_at(uint32_t i) {
+        if (i >= twlen) {
+            fail("twiddle out of range", i);
+            return TwPair{0, 0};
+        }
         return twp[i];
+    }
+    uint32_t tw_base(uint32_t i) { return i; }
+    TwPair tw_ld(uint32_t b, uint32_t c) { return tw_at(b + c); }
+    void tw_ld2(uint32_t b, uint32_t c, TwPair& x, TwPair& y) {
+        if ((b + c) % 2) fail("tw_ld2 misaligned", b + c);
+        x = tw_at(b + c);
+        y = tw_at(b + c + 1);
     }
     void after_local_reads() {}
     void before_scatter() {}
 };
-
-uint32_t* g_dump = nullptr;  // optional: shared state after the scatter
 
 struct Stats {
     double worst = 0, sum = 0;
     long n = 0;
 };
 
+uint32_t* g_dump = nullptr;  // optional: work buffer of every CTA after the forward scatter
+
 // Conflict degree of each warp-wide access = max number of distinct words
-// that map to one bank (remote stores are grouped per destination CTA).
+// (16-byte chunks for the 128-bit stage reads, per quarter warp) that map
+// to one bank.
 void account(EmuCluster& cl, Stats& st) {
-    std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, std::vector<uint32_t>> groups;
-    for (auto& a : cl.log) groups[{a.warp, a.seq, a.kind, a.rank_dst}].push_back(a.addr);
+    static const bool verbose = getenv("NTT_EMU_VERBOSE") != nullptr;
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>, std::vector<uint32_t>>
+        groups;
+    for (auto& a : cl.log) groups[{a.src, a.warp, a.seq, a.kind, a.rank_dst}].push_back(a.addr);
+    double worst_step = 0, sum_step = 0, wk[4] = {0, 0, 0, 0};
+    long n_step = 0;
     for (auto& kv : groups) {
+        const uint32_t kd = std::get<3>(kv.first);
+        const bool vec = kd == 3;
         std::map<uint32_t, std::vector<uint32_t>> banks;
-        for (uint32_t w : kv.second) {
-            auto& v = banks[w % 32];
+        for (uint32_t w0 : kv.second) {
+            const uint32_t w = vec ? w0 / 4 : w0;
+            auto& v = banks[vec ? (w % 8) : (w % 32)];
             bool dup = false;
             for (uint32_t x : v) dup |= (x == w);
             if (!dup) v.push_back(w);
@@ -129,12 +228,20 @@ void account(EmuCluster& cl, Stats& st) {
         st.worst = deg > st.worst ? deg : st.worst;
         st.sum += deg;
         st.n++;
+        worst_step = deg > worst_step ? deg : worst_step;
+        sum_step += deg;
+        n_step++;
+        wk[kd] = deg > wk[kd] ? deg : wk[kd];
     }
+    if (verbose && n_step)
+        fprintf(stderr, "  step: worst %.0f avg %.2f (lds %.0f, sts %.0f, dsmem %.0f, stage128 %.0f)\n",
+                worst_step, sum_step / n_step, wk[0], wk[1], wk[2], wk[3]);
     cl.log.clear();
 }
 
-template <class G, class Arith, bool Fwd>
+template <class G, class Arith, bool Fwd, bool Staged>
 int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::string& err) {
+    using Ctx = EmuCtx<Staged>;
     EmuCluster cl;
     cl.C = G::C;
     cl.smem_words = G::SMEM_WORDS;
@@ -142,20 +249,44 @@ int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::strin
     cl.writes.assign(G::C, std::vector<uint32_t>(G::SMEM_WORDS, 0));
     cl.shadow.assign(G::C, std::vector<uint32_t>(G::SMEM_WORDS, 0));
     cl.rwrites.assign(G::C, std::vector<uint32_t>(G::SMEM_WORDS, 0));
+    cl.writer.assign(G::C, std::vector<uint32_t>(G::SMEM_WORDS, 0xFFFFFFFFu));
     std::vector<uint32_t> gw(1u << G::LOGN, 0);
+    // the kernel's bulk copies of the input slab into each CTA's stage buffer
+    cl.stage.assign(G::C, std::vector<uint32_t>(G::STAGE_WORDS, 0xDEADBEEFu));
+    for (uint32_t r = 0; r < (uint32_t)G::C; ++r) {
+        std::vector<uint32_t> cover(G::STAGE_WORDS, 0);
+        for (uint32_t i = 0; i < slab_copies<G, Fwd>(); ++i) {
+            const SlabCopy c = slab_copy<G, Fwd>(r, i);
+            if ((c.src % 4) || (c.dst % 4) || (c.words % 4) || c.src + c.words > (1u << G::LOGN) ||
+                c.dst + c.words > G::STAGE_WORDS) {
+                err = "bulk copy descriptor out of range or not 16-byte granular";
+                return 1;
+            }
+            for (uint32_t k = 0; k < c.words; ++k) {
+                cl.stage[r][c.dst + k] = limb[c.src + k];
+                cover[c.dst + k]++;
+            }
+        }
+        for (uint32_t lam = 0; lam < G::M; ++lam)
+            if (cover[StageLayout::phys(lam)] != 1) {
+                err = "stage buffer not covered exactly once by the bulk copies";
+                return 1;
+            }
+    }
     auto mk = [&](uint32_t rank) {
-        EmuCtx c{&cl, limb, 1u << G::LOGN, tw, 1u << G::LOGN, q, 2 * q, rank};
+        Ctx c{&cl, limb, 1u << G::LOGN, tw, 1u << G::LOGN, q, 2 * q, rank};
         c.gwrites = &gw;
         return c;
     };
-    using F = Forward<G, Arith, EmuCtx>;
-    using I = Inverse<G, Arith, EmuCtx>;
-    // step runner: run fn for every thread of every CTA
-    auto step = [&](auto fn) {
+    using F = Forward<G, Arith, Ctx>;
+    using I = Inverse<G, Arith, Ctx>;
+    // run fn for every thread of every CTA, then commit the scattered words
+    auto step = [&](auto fn, bool warp_local) {
+        cl.warp_local = warp_local;
         for (auto& w : cl.writes) std::fill(w.begin(), w.end(), 0u);
         for (auto& w : cl.rwrites) std::fill(w.begin(), w.end(), 0u);
         for (uint32_t r = 0; r < (uint32_t)G::C; ++r) {
-            EmuCtx c = mk(r);
+            Ctx c = mk(r);
             for (uint32_t t = 0; t < (uint32_t)G::THREADS; ++t) {
                 c.tid = t;
                 c.seq = 0;
@@ -164,47 +295,49 @@ int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::strin
         }
         for (int r = 0; r < G::C; ++r)
             for (uint32_t w = 0; w < G::SMEM_WORDS; ++w)
-                if (cl.rwrites[r][w]) cl.smem[r][w] = cl.shadow[r][w];
+                if (cl.rwrites[r][w]) {
+                    cl.smem[r][w] = cl.shadow[r][w];
+                    cl.writer[r][w] = 0xFFFFFFFFu;  // scattered words: never warp-local
+                }
         account(cl, st);
     };
-    // every non-pad shared word written exactly once by a store step
+    // every non-pad work-buffer word written exactly once by the last step
     auto check_cover = [&](const char* what) {
         for (int r = 0; r < G::C; ++r)
             for (uint32_t lam = 0; lam < G::M; ++lam)
-                if (cl.writes[r][smem_phys(lam)] != 1) {
-                    if (err.empty())
-                        err = std::string(what) + ": shared word not written exactly once";
+                if (cl.writes[r][G::XW::phys(lam)] != 1) {
+                    if (err.empty()) err = std::string(what) + ": word not written exactly once";
                     return;
                 }
     };
     if (Fwd) {
-        step([](EmuCtx& c, uint32_t t) { F::pass1a(c, t); });
+        step([](Ctx& c, uint32_t t) { F::pass1a(c, t); }, false);
         if (G::K1B > 0) {
             check_cover("pass1a");
-            step([](EmuCtx& c, uint32_t t) { F::pass1b(c, t); });
+            step([](Ctx& c, uint32_t t) { F::pass1b(c, t); }, G::WARP1);
         }
-        check_cover("scatter");
+        check_cover("forward scatter");
         if (g_dump)
             for (int r = 0; r < G::C; ++r)
                 for (uint32_t lam = 0; lam < G::M; ++lam)
-                    g_dump[r * G::M + lam] = cl.smem[r][smem_phys(lam)];
-        step([](EmuCtx& c, uint32_t t) { F::pass2a(c, t); });
+                    g_dump[r * G::M + lam] = cl.smem[r][G::XW::phys(lam)];
+        step([](Ctx& c, uint32_t t) { F::pass2a(c, t); }, false);
         if (G::K2B > 0) {
             check_cover("pass2a");
-            step([](EmuCtx& c, uint32_t t) { F::pass2b(c, t); });
+            step([](Ctx& c, uint32_t t) { F::pass2b(c, t); }, G::WARP2);
         }
     } else {
         if (G::K2B > 0) {
-            step([](EmuCtx& c, uint32_t t) { I::pass2b(c, t); });
+            step([](Ctx& c, uint32_t t) { I::pass2b(c, t); }, false);
             check_cover("pass2b");
         }
-        step([](EmuCtx& c, uint32_t t) { I::pass2a(c, t); });
-        check_cover("scatter");
+        step([](Ctx& c, uint32_t t) { I::pass2a(c, t); }, G::K2B > 0 && G::WARP2);
+        check_cover("inverse scatter");
         if (G::K1B > 0) {
-            step([](EmuCtx& c, uint32_t t) { I::pass1b(c, t); });
+            step([](Ctx& c, uint32_t t) { I::pass1b(c, t); }, false);
             check_cover("pass1b");
         }
-        step([](EmuCtx& c, uint32_t t) { I::pass1a(c, t); });
+        step([](Ctx& c, uint32_t t) { I::pass1a(c, t); }, G::K1B > 0 && G::WARP1);
     }
     for (uint32_t i = 0; i < (1u << G::LOGN); ++i)
         if (gw[i] != 1 && err.empty()) err = "global word not written exactly once";
@@ -212,7 +345,7 @@ int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::strin
     return err.empty() ? 0 : 1;
 }
 
-template <class G>
+template <class G, bool Staged>
 int run_cfg(int fwd, uint32_t* data, const uint32_t* tw_pairs, const uint32_t* q, int limbs,
             double* stats, std::string& err) {
     Stats st;
@@ -221,11 +354,11 @@ int run_cfg(int fwd, uint32_t* data, const uint32_t* tw_pairs, const uint32_t* q
         const TwPair* tw = reinterpret_cast<const TwPair*>(tw_pairs) + l * N;
         int rc;
         if (q[l] < (1u << 30))
-            rc = fwd ? run_limb<G, Lazy4, true>(data + l * N, tw, q[l], st, err)
-                     : run_limb<G, Lazy4, false>(data + l * N, tw, q[l], st, err);
+            rc = fwd ? run_limb<G, Lazy4, true, Staged>(data + l * N, tw, q[l], st, err)
+                     : run_limb<G, Lazy4, false, Staged>(data + l * N, tw, q[l], st, err);
         else
-            rc = fwd ? run_limb<G, Lazy2, true>(data + l * N, tw, q[l], st, err)
-                     : run_limb<G, Lazy2, false>(data + l * N, tw, q[l], st, err);
+            rc = fwd ? run_limb<G, Lazy2, true, Staged>(data + l * N, tw, q[l], st, err)
+                     : run_limb<G, Lazy2, false, Staged>(data + l * N, tw, q[l], st, err);
         if (rc) return rc;
     }
     if (stats) {
@@ -235,17 +368,22 @@ int run_cfg(int fwd, uint32_t* data, const uint32_t* tw_pairs, const uint32_t* q
     return 0;
 }
 
+using RunFn = int (*)(int, uint32_t*, const uint32_t*, const uint32_t*, int, double*,
+                      std::string&);
 struct Entry {
     int v[6];
     int threads;
     unsigned smem;
-    int (*fn)(int, uint32_t*, const uint32_t*, const uint32_t*, int, double*, std::string&);
+    RunFn staged, direct;
 };
 
-#define EMU_ENTRY(N, CL, R1, EB, K1A, K2A)                                              \
-    {{N, CL, R1, EB, K1A, K2A}, Geometry<N, CL, R1, EB, K1A, K2A>::THREADS,             \
-     Geometry<N, CL, R1, EB, K1A, K2A>::SMEM_BYTES,                                     \
-     &run_cfg<Geometry<N, CL, R1, EB, K1A, K2A>>},
+#define EMU_G(N, CL, R1, EB, K1A, K2A) Geometry<N, CL, R1, EB, K1A, K2A>
+#define EMU_ENTRY(N, CL, R1, EB, K1A, K2A)                                                 \
+    {{N, CL, R1, EB, K1A, K2A},                                                            \
+     EMU_G(N, CL, R1, EB, K1A, K2A)::THREADS,                                              \
+     EMU_G(N, CL, R1, EB, K1A, K2A)::SMEM_BYTES,                                           \
+     &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A), true>,                                       \
+     &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A), false>},
 const Entry kEntries[] = {NTTB_CFG_ALL(EMU_ENTRY)};
 std::string g_err;
 
@@ -259,10 +397,12 @@ void emu_config(int i, int* out8) {
     out8[7] = (int)kEntries[i].smem;
 }
 // data: limbs * N words in place; tw_pairs: limbs * N (w, w') pairs.
-int emu_transform(int i, int fwd, uint32_t* data, const uint32_t* tw_pairs, const uint32_t* q,
+// mode bit 0: forward (else inverse); bit 1: direct input (else staged).
+int emu_transform(int i, int mode, uint32_t* data, const uint32_t* tw_pairs, const uint32_t* q,
                   int limbs, double* stats) {
     g_err.clear();
-    return kEntries[i].fn(fwd, data, tw_pairs, q, limbs, stats, g_err);
+    RunFn fn = (mode & 2) ? kEntries[i].direct : kEntries[i].staged;
+    return fn(mode & 1, data, tw_pairs, q, limbs, stats, g_err);
 }
 const char* emu_last_error() { return g_err.c_str(); }
 void emu_set_dump(uint32_t* p) { g_dump = p; }
