@@ -49,6 +49,7 @@ def roundtrip_check(torch, nb, logN, mods, x, plan=None):
     torch.cuda.synchronize()
     expect = np.stack([x[i] % np.uint32(q) for i, (q, _) in enumerate(mods)])
     assert np.array_equal(host(d), expect), "inverse mismatch"
+    assert p.check() == 0  # no bounded wait expired on the device"
 
 
 def test_config1_baseline_moduli(torch_cuda, nb):
@@ -83,15 +84,29 @@ def test_small_sizes(torch_cuda, nb, logN):
     roundtrip_check(torch_cuda, nb, logN, mods, x)
 
 
-def test_every_compiled_config(torch_cuda, nb):
+@pytest.mark.parametrize("schedule", [0, 1], ids=["direct", "staged"])
+def test_every_compiled_config(torch_cuda, nb, schedule):
+    """Every compiled configuration under both schedules, 30/31-bit moduli,
+    several polynomials per launch (the staged schedule prefetches across
+    limbs of one cluster's chunk)."""
     cfgs = nb.kernel_configs()
     for idx, c in enumerate(cfgs):
         for bits in (30, 31):
             mods = moduli_set(c.logN, 3, bits)
             p = nb.Plan(c.logN, mods)
             p.force_config(idx, idx)
+            p.set_schedule(schedule)
             x = O.uniform_limbs(c.logN, [q for q, _ in mods], idx)
             roundtrip_check(torch_cuda, nb, c.logN, mods, x, plan=p)
+            polys = 5
+            xs = np.stack([O.uniform_limbs(c.logN, [q for q, _ in mods], 100 * idx + k)
+                           for k in range(polys)])
+            d = dev(torch_cuda, xs)
+            p.forward_many(d, polys)
+            p.inverse_many(d, polys)
+            torch_cuda.cuda.synchronize()
+            assert np.array_equal(host(d).reshape(xs.shape), xs)
+            assert p.check() == 0
 
 
 @pytest.mark.parametrize("logN", [5, 12, 16, 17])
