@@ -1,0 +1,92 @@
+/*
+ * ntt_b200 ragged batches (C ABI): many polynomials of different sizes,
+ * limb counts, modulus chains and operations in ONE persistent launch.
+ *
+ * No reference counterpart: the reference transforms one polynomial per
+ * launch_ntt<LC> / launch_intt<LC> call (src/v04_montgomery.cu:603-658) with
+ * a compile-time logN.  A batch replaces a host loop of such calls.  Each
+ * (polynomial, limb) becomes a tile; resident thread-block clusters drain a
+ * device-side queue of tile groups.  Per tile the results are bit-identical
+ * to ntt_forward / ntt_inverse of a plan with the same modulus.
+ *
+ * Operations (per job, on caller-owned device memory, limb-major
+ * data[limb * 2^logN + i], 16-byte aligned):
+ *   NTT_OP_FORWARD   data <- NTT(data)              (as ntt_forward)
+ *   NTT_OP_INVERSE   data <- INTT(data)             (as ntt_inverse)
+ *   NTT_OP_MULTIPLY  data <- a * data  negacyclic, mod each q, normal domain
+ *                    in and out: INTT(NTT(a) (.) NTT(data)) with (.) the
+ *                    pointwise Montgomery product; a = operand, read only.
+ * Twiddle tables are generated on the device once per (device, logN,
+ * modulus) and kept resident in a process-wide registry shared by all
+ * batches.  Jobs of one batch must not overlap in memory (operands may be
+ * shared).  logN 12..17.
+ */
+#ifndef NTT_B200_BATCH_H
+#define NTT_B200_BATCH_H
+#include "ntt_b200.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NTT_OP_FORWARD 0
+#define NTT_OP_INVERSE 1
+#define NTT_OP_MULTIPLY 2
+
+#define NTT_BATCH_MIN_LOGN 12
+#define NTT_BATCH_MAX_LOGN 17
+
+typedef struct ntt_job {
+    int op;                        /* NTT_OP_* */
+    int logN;                      /* 12..17 */
+    int limbs;                     /* >= 1 */
+    const ModulusConfig* moduli;   /* host array [limbs]: the job's modulus chain */
+    uint32_t* data;                /* device, limbs * 2^logN words, in place */
+    const uint32_t* operand;       /* NTT_OP_MULTIPLY: the other factor (device, same
+                                      shape); otherwise NULL */
+} ntt_job_t;
+
+typedef struct ntt_batch_options {
+    int cluster_ctas; /* CTAs per cluster: 8, 16, or 0 = automatic (16 when a
+                         job has logN 17, else 8) */
+    int use_graph;    /* nonzero: ntt_batch_run replays a CUDA graph (default);
+                         zero: a plain kernel launch */
+    int max_clusters; /* cap on resident clusters (0 = as many as fit) */
+} ntt_batch_options_t;
+
+typedef struct ntt_batch_info {
+    int jobs;
+    int tiles;          /* (polynomial, limb) tiles */
+    int groups;         /* tile groups in the device queue */
+    int cluster_ctas;
+    int clusters;       /* clusters launched (persistent) */
+    int multiply;       /* nonzero: the kernel variant with multiply tiles */
+    uint32_t smem_bytes;/* dynamic shared memory per CTA */
+    size_t device_bytes;/* descriptors owned by the batch */
+} ntt_batch_info_t;
+
+typedef struct ntt_batch ntt_batch_t;
+
+/* Validates every job (moduli as ntt_plan_create does), generates missing
+ * twiddle tables on the current device, packs the tiles into groups and
+ * uploads the descriptors.  Synchronous.  opts may be NULL. */
+NTT_API ntt_status_t ntt_batch_create(const ntt_job_t* jobs, int count,
+                                      const ntt_batch_options_t* opts, ntt_batch_t** out);
+/* One persistent launch over every tile of the batch on `stream` (the
+ * descriptors stay valid, so a batch can be run again on new contents of
+ * the same buffers).  Runs of one batch must not overlap in time. */
+NTT_API ntt_status_t ntt_batch_run(ntt_batch_t* batch, ntt_stream_t stream);
+NTT_API ntt_status_t ntt_batch_get_info(const ntt_batch_t* batch, ntt_batch_info_t* out);
+/* Frees the batch's descriptors (waits for its launches to finish). */
+NTT_API ntt_status_t ntt_batch_destroy(ntt_batch_t* batch);
+/* create + run + wait + destroy. */
+NTT_API ntt_status_t ntt_batch_submit(const ntt_job_t* jobs, int count, ntt_stream_t stream);
+
+/* Resident twiddle-table registry: bytes held on the current device, and a
+ * release of every table no live batch or server uses. */
+NTT_API size_t ntt_tables_device_bytes(void);
+NTT_API void ntt_tables_trim(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

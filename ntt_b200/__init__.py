@@ -402,3 +402,109 @@ def autotune_forget():
 
 def autotune_reload():
     _lib.ntt_autotune_reload()
+
+
+# ---------------------------------------------------------------------------
+# ragged batches (include/ntt_b200_batch.h)
+# ---------------------------------------------------------------------------
+
+OP_FORWARD = 0
+OP_INVERSE = 1
+OP_MULTIPLY = 2
+BATCH_MIN_LOGN = 12
+BATCH_MAX_LOGN = 17
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_int), ("logN", ctypes.c_int), ("limbs", ctypes.c_int),
+                ("moduli", ctypes.POINTER(ModulusConfig)), ("data", _vp), ("operand", _vp)]
+
+
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("cluster_ctas", ctypes.c_int), ("use_graph", ctypes.c_int),
+                ("max_clusters", ctypes.c_int)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("jobs", ctypes.c_int), ("tiles", ctypes.c_int), ("groups", ctypes.c_int),
+                ("cluster_ctas", ctypes.c_int), ("clusters", ctypes.c_int),
+                ("multiply", ctypes.c_int), ("smem_bytes", ctypes.c_uint32),
+                ("device_bytes", ctypes.c_size_t)]
+
+
+_sig("ntt_batch_create", _st, ctypes.POINTER(Job), ctypes.c_int, ctypes.POINTER(BatchOptions),
+     ctypes.POINTER(_vp))
+_sig("ntt_batch_run", _st, _vp, _vp)
+_sig("ntt_batch_get_info", _st, _vp, ctypes.POINTER(BatchInfo))
+_sig("ntt_batch_destroy", _st, _vp)
+_sig("ntt_batch_submit", _st, ctypes.POINTER(Job), ctypes.c_int, _vp)
+_sig("ntt_tables_device_bytes", ctypes.c_size_t)
+_sig("ntt_tables_trim", None)
+
+
+def _job_array(jobs: Sequence) -> tuple:
+    """jobs: sequence of (op, logN, moduli, data, operand-or-None)."""
+    keep = []
+    arr = (Job * max(1, len(jobs)))()
+    for i, (op, logN, moduli, data, operand) in enumerate(jobs):
+        m, n = _moduli_array(moduli)
+        keep.append(m)
+        arr[i] = Job(op, logN, n, ctypes.cast(m, ctypes.POINTER(ModulusConfig)), _ptr(data),
+                     _ptr(operand))
+    return arr, keep
+
+
+class Batch:
+    """A ragged set of jobs run by one persistent launch (CUDA-graph replay
+    by default).  jobs: sequence of (op, logN, moduli, data, operand) with
+    op in OP_FORWARD / OP_INVERSE / OP_MULTIPLY, data (and operand) device
+    buffers of limbs * 2^logN uint32 words."""
+
+    def __init__(self, jobs: Sequence, cluster_ctas: int = 0, use_graph: bool = True,
+                 max_clusters: int = 0):
+        arr, self._keep = _job_array(jobs)
+        opts = BatchOptions(cluster_ctas, 1 if use_graph else 0, max_clusters)
+        h = _vp()
+        _check(_lib.ntt_batch_create(arr, len(jobs), ctypes.byref(opts), ctypes.byref(h)),
+               "ntt_batch_create")
+        self._h = h
+
+    def run(self, stream=None):
+        _check(_lib.ntt_batch_run(self._h, _stream(stream)), "ntt_batch_run")
+
+    @property
+    def info(self) -> BatchInfo:
+        i = BatchInfo()
+        _check(_lib.ntt_batch_get_info(self._h, ctypes.byref(i)), "ntt_batch_get_info")
+        return i
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.ntt_batch_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def batch_submit(jobs: Sequence, stream=None):
+    """Create, run, wait for and destroy a one-off batch."""
+    arr, keep = _job_array(jobs)
+    _check(_lib.ntt_batch_submit(arr, len(jobs), _stream(stream)), "ntt_batch_submit")
+
+
+def tables_device_bytes() -> int:
+    return _lib.ntt_tables_device_bytes()
+
+
+def tables_trim():
+    _lib.ntt_tables_trim()

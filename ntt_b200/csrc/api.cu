@@ -277,6 +277,19 @@ ntt_status_t validate_modulus(int logN, ModulusConfig m, ModulusRuntime* rt) {
     return NTT_OK;
 }
 
+ntt_status_t twiddle_gen_inputs(int logN, ModulusConfig m, TwGenLimb* fwd, TwGenLimb* inv) {
+    ModulusRuntime rt;
+    if (ntt_status_t st = validate_modulus(logN, m, &rt)) return st;
+    const uint32_t q = rt.qi, R = hm::r_mod(q);
+    const uint32_t Rinv = hm::powmod(R, q - 2, q);
+    const uint32_t c = hm::mulmod(rt.degree_inv, Rinv, q);
+    const uint32_t w1 = hm::powmod(rt.psi, hm::bitrev(1, logN), q);
+    const uint32_t w1i = hm::powmod(rt.psi_inv, hm::bitrev(1, logN), q);
+    *fwd = TwGenLimb{q, rt.q_inv, R, rt.r2, rt.psi, R, hm::mulmod(w1, R, q)};
+    *inv = TwGenLimb{q, rt.q_inv, R, rt.r2, rt.psi_inv, c, hm::mulmod(w1i, c, q)};
+    return NTT_OK;
+}
+
 ntt_status_t check_transform(int logN, const TransformConfig* t) {
     if (!t) return NTT_OK;
     const PhaseConfig* ph[4] = {&t->ntt_phase1, &t->ntt_phase2, &t->intt_phase1, &t->intt_phase2};
@@ -402,16 +415,8 @@ ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int limbs,
     std::vector<uint32_t> qh(limbs);
     const uint32_t N = 1u << logN;
     for (int l = 0; l < limbs; ++l) {
-        ModulusRuntime rt;
-        if (ntt_status_t st = validate_modulus(logN, moduli[l], &rt)) return st;
-        const uint32_t q = rt.qi, R = hm::r_mod(q);
-        const uint32_t Rinv = hm::powmod(R, q - 2, q);
-        const uint32_t c = hm::mulmod(rt.degree_inv, Rinv, q);
-        const uint32_t w1 = hm::powmod(rt.psi, hm::bitrev(1, logN), q);
-        const uint32_t w1i = hm::powmod(rt.psi_inv, hm::bitrev(1, logN), q);
-        gf[l] = TwGenLimb{q, rt.q_inv, R, rt.r2, rt.psi, R, hm::mulmod(w1, R, q)};
-        gi[l] = TwGenLimb{q, rt.q_inv, R, rt.r2, rt.psi_inv, c, hm::mulmod(w1i, c, q)};
-        qh[l] = q;
+        if (ntt_status_t st = twiddle_gen_inputs(logN, moduli[l], &gf[l], &gi[l])) return st;
+        qh[l] = gf[l].q;
     }
     auto* p = new ntt_plan();
     p->logN = logN;

@@ -136,6 +136,17 @@ struct Lazy2 {  // q < 2^31
     }
 };
 
+// Montgomery product x*y*2^-32 mod q (REDC, as the reference's mont_mul,
+// src/v04_montgomery.cu:110-123), for x, y < q < 2^31 and qinv = -q^{-1}
+// mod 2^32; canonical output.  Used once per coefficient by the fused
+// multiply (pointwise product of two Montgomery-domain spectra).
+NTT_HD uint32_t mont_mul(uint32_t x, uint32_t y, uint32_t q, uint32_t qinv) {
+    const uint64_t t = (uint64_t)x * y;
+    const uint32_t m = (uint32_t)t * qinv;
+    const uint32_t u = (uint32_t)((t + (uint64_t)m * q) >> 32);
+    return csub(u, q);
+}
+
 // ---- host-side helpers for table construction ------------------------------
 
 inline uint32_t shoup_companion(uint32_t w, uint32_t q) {

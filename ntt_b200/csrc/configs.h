@@ -14,7 +14,7 @@
 
 #define NTTB_CFG_N10(X) X(10, 0, 5, 5, 5, 5)
 #define NTTB_CFG_N11(X) X(11, 0, 6, 5, 1, 5)
-#define NTTB_CFG_N12(X) X(12, 0, 7, 5, 3, 5)
+#define NTTB_CFG_N12(X) X(12, 0, 7, 5, 3, 5) X(12, 0, 6, 4, 3, 3)
 #define NTTB_CFG_N13(X) X(13, 0, 8, 5, 3, 5)
 #define NTTB_CFG_N14(X) X(14, 0, 9, 5, 4, 5) X(14, 1, 9, 5, 4, 5)
 #define NTTB_CFG_N15(X) X(15, 1, 10, 5, 5, 5) X(15, 2, 8, 5, 3, 4)

@@ -108,8 +108,10 @@ struct DevCtx {
         z = t.z;
         w = t.w;
     }
-    __device__ __forceinline__ void g_st(uint32_t* b, uint32_t c, uint32_t v) const { b[c] = v; }
-    __device__ __forceinline__ void g_st4(uint32_t* b, uint32_t c, uint32_t x, uint32_t y,
+    // transform output: in place
+    __device__ __forceinline__ uint32_t* o_base(uint32_t o) const { return g + o; }
+    __device__ __forceinline__ void o_st(uint32_t* b, uint32_t c, uint32_t v) const { b[c] = v; }
+    __device__ __forceinline__ void o_st4(uint32_t* b, uint32_t c, uint32_t x, uint32_t y,
                                           uint32_t z, uint32_t w) const {
         *reinterpret_cast<uint4*>(b + c) = make_uint4(x, y, z, w);
     }
@@ -172,6 +174,16 @@ struct DevCtx {
     __device__ __forceinline__ void before_scatter() const {
         if constexpr (C > 1) cluster_wait_acquire();
     }
+    // Phase boundary: after the scatter, every scattered word must be visible
+    // to its owner before phase 2 (forward) / phase 1 (inverse) reads it.
+    __device__ __forceinline__ void phase_sync() const {
+        if constexpr (C > 1) {
+            cluster_arrive_release();
+            cluster_wait_acquire();
+        } else {
+            __syncthreads();
+        }
+    }
 };
 
 // Exchange between two register passes of one phase: a warp barrier when
@@ -180,18 +192,6 @@ template <bool WarpLocal>
 __device__ __forceinline__ void pass_sync() {
     if constexpr (WarpLocal) __syncwarp();
     else __syncthreads();
-}
-
-// Phase boundary: after the scatter, every scattered word must be visible
-// to its owner before phase 2 (forward) / phase 1 (inverse) reads it.
-template <class G>
-__device__ __forceinline__ void cta_or_cluster_sync() {
-    if constexpr (G::C > 1) {
-        cluster_arrive_release();
-        cluster_wait_acquire();
-    } else {
-        __syncthreads();
-    }
 }
 
 // Issue the bulk copies of job `job`'s input slab into the stage buffer
@@ -210,16 +210,16 @@ __device__ __forceinline__ void issue_slab(const FusedArgs& a, uint32_t job, uin
 }
 
 // One limb transform; `prefetch()` is called once the stage buffer is free.
-template <class G, bool Staged, class Arith, class Pre>
-__device__ __forceinline__ void fused_forward_body(DevCtx<G::C, Staged>& ctx, Pre&& prefetch) {
-    using F = Forward<G, Arith, DevCtx<G::C, Staged>>;
+template <class G, class Arith, class Ctx, class Pre>
+__device__ __forceinline__ void fused_forward_body(Ctx& ctx, Pre&& prefetch) {
+    using F = Forward<G, Arith, Ctx>;
     const uint32_t tid = threadIdx.x;
     F::pass1a(ctx, tid);
     if constexpr (G::K1B > 0) {
         pass_sync<G::WARP1>();
         F::pass1b(ctx, tid);
     }
-    cta_or_cluster_sync<G>();
+    ctx.phase_sync();
     prefetch();  // every warp has read the stage buffer
     F::pass2a(ctx, tid);
     if constexpr (G::K2B > 0) {
@@ -228,16 +228,16 @@ __device__ __forceinline__ void fused_forward_body(DevCtx<G::C, Staged>& ctx, Pr
     }
 }
 
-template <class G, bool Staged, class Arith, class Pre>
-__device__ __forceinline__ void fused_inverse_body(DevCtx<G::C, Staged>& ctx, Pre&& prefetch) {
-    using I = Inverse<G, Arith, DevCtx<G::C, Staged>>;
+template <class G, class Arith, class Ctx, class Pre>
+__device__ __forceinline__ void fused_inverse_body(Ctx& ctx, Pre&& prefetch) {
+    using I = Inverse<G, Arith, Ctx>;
     const uint32_t tid = threadIdx.x;
     if constexpr (G::K2B > 0) {
         I::pass2b(ctx, tid);
         pass_sync<G::WARP2>();
     }
     I::pass2a(ctx, tid);
-    cta_or_cluster_sync<G>();
+    ctx.phase_sync();
     prefetch();  // every warp has read the stage buffer
     if constexpr (G::K1B > 0) {
         I::pass1b(ctx, tid);
@@ -289,11 +289,11 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedA
                 if (job + 1 < j1) issue_slab<G, Fwd>(a, job + 1, rank, stage_sa, mbar_sa);
         };
         if (ctx.q < (1u << 30)) {
-            if constexpr (Fwd) fused_forward_body<G, Staged, Lazy4>(ctx, prefetch);
-            else fused_inverse_body<G, Staged, Lazy4>(ctx, prefetch);
+            if constexpr (Fwd) fused_forward_body<G, Lazy4>(ctx, prefetch);
+            else fused_inverse_body<G, Lazy4>(ctx, prefetch);
         } else {
-            if constexpr (Fwd) fused_forward_body<G, Staged, Lazy2>(ctx, prefetch);
-            else fused_inverse_body<G, Staged, Lazy2>(ctx, prefetch);
+            if constexpr (Fwd) fused_forward_body<G, Lazy2>(ctx, prefetch);
+            else fused_inverse_body<G, Lazy2>(ctx, prefetch);
         }
         __syncthreads();  // the work buffer is rewritten by the next job
     }

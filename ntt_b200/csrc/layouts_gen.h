@@ -38,6 +38,15 @@ struct LayoutTable<12, 0, 7, 5, 3, 5> {
 };
 
 template <>
+struct LayoutTable<12, 0, 6, 4, 3, 3> {
+    static constexpr int XW[5] = {6, 1, 8, 4, 4219};
+    static constexpr uint32_t lanes_P1A = 0x3eu;
+    static constexpr uint32_t lanes_P1B = 0x3eu;
+    static constexpr uint32_t lanes_P2A = 0x1c6u;
+    static constexpr uint32_t lanes_P2B = 0x1f0u;
+};
+
+template <>
 struct LayoutTable<13, 0, 8, 5, 3, 5> {
     static constexpr int XW[5] = {5, 1, 13, 0, 8447};
     static constexpr uint32_t lanes_P1A = 0x7cu;

@@ -415,22 +415,24 @@ NTT_HD void load_global(Ctx& ctx, uint32_t (&v)[L::E], uint32_t gbase) {
     }
 }
 
+// The transform's output goes through the context's o_* interface (global
+// memory for a plain transform; a fused caller may redirect it).
 template <class L, uint32_t Lim, class GMap, class Ctx, class ValFn>
 NTT_HD void store_global(Ctx& ctx, uint32_t (&v)[L::E], uint32_t gbase, ValFn fin) {
-    auto gb = ctx.g_base(gbase);
+    auto gb = ctx.o_base(gbase);
     if constexpr (use_vec4<L, Lim>()) {
         ct_for<L::E>([&](auto R) {
             constexpr int r = decltype(R)::value;
             constexpr uint32_t o = L::off(r);
             if constexpr ((o & 3u) == 0) {
-                ctx.g_st4(gb, GMap::map(o), fin(v[L::reg_of(o)]), fin(v[L::reg_of(o + 1)]),
+                ctx.o_st4(gb, GMap::map(o), fin(v[L::reg_of(o)]), fin(v[L::reg_of(o + 1)]),
                           fin(v[L::reg_of(o + 2)]), fin(v[L::reg_of(o + 3)]));
             }
         });
     } else {
         ct_for<L::E>([&](auto R) {
             constexpr int r = decltype(R)::value;
-            ctx.g_st(gb, GMap::map(L::off(r)), fin(v[r]));
+            ctx.o_st(gb, GMap::map(L::off(r)), fin(v[r]));
         });
     }
 }

@@ -6,6 +6,7 @@
 #include "../../include/ntt_b200_tune.h"
 #include "configs.h"
 #include "fused_kernel.cuh"
+#include "twiddle.h"
 
 namespace nttb {
 
@@ -25,6 +26,9 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule);
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
                           int schedule);
 ntt_status_t validate_modulus(int logN, ModulusConfig m, ModulusRuntime* rt);
+// Validates m and fills the twiddle-generation inputs of both directions
+// (entries 0/1 carry the folded Montgomery / N^{-1} R^{-1} factors).
+ntt_status_t twiddle_gen_inputs(int logN, ModulusConfig m, TwGenLimb* fwd, TwGenLimb* inv);
 // One launch over `polys` polynomials of `limbs` limbs (cfg == nullptr: the
 // single-CTA small-size kernel).  status: optional device error word.
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,

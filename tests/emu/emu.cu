@@ -91,19 +91,21 @@ struct EmuCtx {
         z = g[o + 2];
         w = g[o + 3];
     }
-    void g_st(uint32_t b, uint32_t c, uint32_t v) {
+    // transform output (in place)
+    uint32_t o_base(uint32_t o) { return o; }
+    void o_st(uint32_t b, uint32_t c, uint32_t v) {
         const uint32_t o = b + c;
         if (o >= glen) {
-            fail("g_st out of range", o);
+            fail("o_st out of range", o);
             return;
         }
         g[o] = v;
         (*gwrites)[o]++;
     }
-    void g_st4(uint32_t b, uint32_t c, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+    void o_st4(uint32_t b, uint32_t c, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
         const uint32_t o = b + c;
         if (o % 4 || o + 3 >= glen) {
-            fail("g_st4 out of range or misaligned", o);
+            fail("o_st4 out of range or misaligned", o);
             return;
         }
         g[o] = x;

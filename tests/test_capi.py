@@ -122,3 +122,38 @@ def test_invalid_plan_arguments():
     with pytest.raises(nb.NttError) as e:
         nb.Plan(16, [(974258177, 3)], bad)
     assert e.value.name == "NTT_ERR_INVALID_ARGUMENT"
+
+
+def test_batch_job_validation_without_device():
+    """Job-level checks run before any device call (status codes, no exit)."""
+    mods = [(m.qi, m.primitive_root) for m in nb.find_moduli(12, 2, 1 << 29)]
+    cases = [
+        ((7, 12, mods, 0x1000, None), "NTT_ERR_INVALID_ARGUMENT"),    # unknown op
+        ((nb.OP_FORWARD, 11, mods, 0x1000, None), "NTT_ERR_UNSUPPORTED"),
+        ((nb.OP_FORWARD, 18, mods, 0x1000, None), "NTT_ERR_UNSUPPORTED"),
+        ((nb.OP_FORWARD, 12, [], 0x1000, None), "NTT_ERR_INVALID_ARGUMENT"),
+        ((nb.OP_FORWARD, 12, mods, 0x1004, None), "NTT_ERR_MISALIGNED"),
+        ((nb.OP_MULTIPLY, 12, mods, 0x1000, None), "NTT_ERR_INVALID_ARGUMENT"),
+        ((nb.OP_MULTIPLY, 12, mods, 0x1000, 0x2008), "NTT_ERR_MISALIGNED"),
+    ]
+    for job, name in cases:
+        with pytest.raises(nb.NttError) as e:
+            nb.Batch([job])
+        assert e.value.name == name, job
+    with pytest.raises(nb.NttError) as e:
+        nb.Batch([(nb.OP_FORWARD, 12, mods, 0x1000, None)], cluster_ctas=4)
+    assert e.value.name == "NTT_ERR_INVALID_ARGUMENT"
+
+
+def test_ragged_mix_is_seeded():
+    from ntt_b200 import mixes
+    a = mixes.ragged_mix(seed=3, count=50, logn=range(12, 17), limbs=(1, 48))
+    b = mixes.ragged_mix(seed=3, count=50, logn=range(12, 17), limbs=(1, 48))
+    assert [(j.op, j.logN, j.moduli) for j in a] == [(j.op, j.logN, j.moduli) for j in b]
+    for j in a:
+        assert 12 <= j.logN <= 16 and 1 <= j.limbs <= 48
+        qs = [q for q, _ in j.moduli]
+        assert qs == sorted(qs) and len(set(qs)) == len(qs)
+        for q, g in j.moduli:
+            assert (q - 1) % (2 << j.logN) == 0 and (1 << 29) < q < (1 << 30)
+    assert len({tuple(j.moduli) for j in a}) > 40  # chains differ between polynomials
