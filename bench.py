@@ -42,12 +42,17 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-steps", type=int, default=20)
+    ap.add_argument("--plain-steps", type=int, default=5)
     return ap.parse_args()
 
 
 def moduli():
-    from oracle import oracle as O  # moduli search is host logic shared with the tests
-    return O.ascending_primes(LOGN, LIMBS, FIRST_Q)
+    """The 16 ascending primes q == 1 (mod 2^17) from 974258177 (the library's
+    own search; the tests check it against the oracle's)."""
+    import ntt_b200 as nb
+    return [(m.qi, m.primitive_root) for m in nb.find_moduli(LOGN, LIMBS, FIRST_Q)]
 
 
 # ---------------------------------------------------------------------------
@@ -59,7 +64,7 @@ def cpu_roundtrip_rate(seconds, threads):
     on one 2^16 x 16 polynomial per repetition, forward + inverse, limbs
     split over `threads` host threads; repeated for about `seconds`."""
     from oracle import oracle as O
-    mods = moduli()
+    mods = O.ascending_primes(LOGN, LIMBS, FIRST_Q)
     T = O.LimbTables(LOGN, mods)
     x = O.uniform_limbs(LOGN, T.q, SEED)
     R = O.ref_lib()
@@ -185,7 +190,6 @@ def run_ours(args):
     N = 1 << LOGN
     P = args.polys
     words = P * LIMBS * N
-    from oracle import oracle as O
     q = np.array([m[0] for m in mods], dtype=np.uint64)
     rng = np.random.default_rng(SEED + rank)
     x = rng.integers(0, q[None, :, None], size=(P, LIMBS, N), dtype=np.uint64).astype(np.uint32)
@@ -202,15 +206,9 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # correctness spot check of the timed path (limb 0 and 15 of polynomial 0)
+    # sanity check of the timed path (bit-exact parity is the tests' job)
     with torch.cuda.stream(stream):
         plan.forward_many(d, P, 0, stream=sh)
-    stream.synchronize()
-    T = O.LimbTables(LOGN, [mods[0], mods[15]])
-    got = d[: LIMBS * N].cpu().numpy().view(np.uint32).reshape(LIMBS, N)[[0, 15]]
-    if not np.array_equal(got, T.forward_mont(x[0][[0, 15]])):
-        raise RuntimeError("forward output differs from the oracle")
-    with torch.cuda.stream(stream):
         plan.inverse_many(d, P, 0, stream=sh)
     stream.synchronize()
     if not torch.equal(d, host_in.cuda()):
@@ -323,6 +321,10 @@ def run_ours(args):
                                "smem_bytes": info.smem_bytes,
                                "phases": [info.effective.ntt_phase1.as_tuple(),
                                           info.effective.ntt_phase2.as_tuple()]}
+    if not args.no_batched:
+        out["batched"] = bench_batched(args, torch, nb, stream)
+        out["gpu_launches_batched"] = 2 * (args.batched_steps + args.plain_steps *
+                                           out["batched"]["polynomials"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, kind, reps, el = cpu_roundtrip_rate(args.cpu_seconds, threads)
@@ -335,6 +337,85 @@ def run_ours(args):
     plan.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+RAGGED = dict(seed=SEED, count=256, logn=tuple(range(12, 17)), limbs=(1, 48), bits=(30,))
+
+
+def device_time(torch, stream, fn, steps, warmup):
+    """Average device time (ms) of fn() over `steps` runs on `stream` after
+    `warmup` untimed runs (CUDA events on the launching stream)."""
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            fn()
+    stream.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+    stream.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def bench_batched(args, torch, nb, stream):
+    """Ragged batch: 256 polynomials, logN uniform in 12..16, limbs uniform
+    in 1..48, each with its own chain of 30-bit primes, uniform [0, q)
+    coefficients.  Step = forward + inverse of every polynomial.  Batched
+    form: two persistent launches (CUDA-graph replays); plain form: one
+    ntt_forward + one ntt_inverse call per polynomial (512 launches)."""
+    from ntt_b200 import mixes
+    jobs = mixes.ragged_mix(**RAGGED)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    data = [mixes.uniform_device(torch, j, g) for j in jobs]
+    orig = [x.clone() for x in data]
+    limbs = sum(j.limbs for j in jobs)
+    words = sum(j.words for j in jobs)
+    sh = stream.cuda_stream
+    plans = [nb.Plan(j.logN, j.moduli) for j in jobs]
+
+    def plain():
+        for p, x in zip(plans, data):
+            p.forward(x, sh)
+            p.inverse(x, sh)
+
+    bf = nb.Batch([(nb.OP_FORWARD, j.logN, j.moduli, x, None) for j, x in zip(jobs, data)])
+    bi = nb.Batch([(nb.OP_INVERSE, j.logN, j.moduli, x, None) for j, x in zip(jobs, data)])
+
+    def batched():
+        bf.run(sh)
+        bi.run(sh)
+
+    w = max(3, args.warmup if args.warmup < 10 else 10)
+    plain_ms = device_time(torch, stream, plain, args.plain_steps, w)
+    batch_ms = device_time(torch, stream, batched, args.batched_steps, w)
+    for x, o in zip(data, orig):  # every step is a roundtrip: data must be unchanged
+        if not torch.equal(x, o):
+            raise RuntimeError("batched / plain roundtrips changed the data")
+    info = bf.info
+    res = {
+        "workload": "256 ragged polynomials: logN uniform 12..16, limbs uniform 1..48, own "
+                    "chains of 30-bit primes q=1 mod 2N, uniform [0,q) coefficients; step = "
+                    "forward + inverse of every polynomial",
+        "polynomials": len(jobs), "limbs": limbs, "bytes": 4 * words,
+        "value": 2 * limbs / (batch_ms / 1000.0), "unit": "limb-NTT/s",
+        "ms_per_step": batch_ms, "launches_per_step": 2,
+        "plain_per_call": {"value": 2 * limbs / (plain_ms / 1000.0), "unit": "limb-NTT/s",
+                           "ms_per_step": plain_ms, "launches_per_step": 2 * len(jobs)},
+        "speedup_vs_plain": plain_ms / batch_ms,
+        "kernel": {"cluster_ctas": info.cluster_ctas, "clusters": info.clusters,
+                   "groups": info.groups, "smem_bytes": info.smem_bytes},
+        "steps": args.batched_steps, "plain_steps": args.plain_steps, "warmup": w,
+        "l2": f"{4 * words >> 20} MiB of inputs > 126 MB L2",
+    }
+    bf.close()
+    bi.close()
+    for p in plans:
+        p.close()
+    return res
 
 
 def main():

@@ -508,3 +508,138 @@ def tables_device_bytes() -> int:
 
 def tables_trim():
     _lib.ntt_tables_trim()
+
+
+# ---------------------------------------------------------------------------
+# serving loop (include/ntt_b200_serve.h)
+# ---------------------------------------------------------------------------
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_int), ("logN", ctypes.c_int), ("limbs", ctypes.c_int),
+                ("moduli", ctypes.POINTER(ModulusConfig)), ("input", _vp), ("operand", _vp),
+                ("operand_handle", ctypes.c_uint64), ("output", _vp)]
+
+
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("streams", ctypes.c_int),
+                ("max_round_tiles", ctypes.c_int), ("cluster_ctas", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("rounds", ctypes.c_uint64),
+                ("mean_round_requests", ctypes.c_double), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("elapsed_s", ctypes.c_double),
+                ("limb_ntt_per_s", ctypes.c_double), ("budget_bytes", ctypes.c_size_t),
+                ("arena_peak_bytes", ctypes.c_size_t), ("resident_bytes", ctypes.c_size_t),
+                ("table_bytes", ctypes.c_size_t)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+_sig("ntt_server_create", _st, ctypes.POINTER(ServerOptions), ctypes.POINTER(_vp))
+_sig("ntt_server_submit", _st, _vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64))
+_sig("ntt_server_poll", _st, _vp, ctypes.c_uint64)
+_sig("ntt_server_wait", _st, _vp, ctypes.c_uint64, ctypes.c_double)
+_sig("ntt_server_latency_ms", ctypes.c_double, _vp, ctypes.c_uint64)
+_sig("ntt_server_put", _st, _vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64))
+_sig("ntt_server_drop", _st, _vp, ctypes.c_uint64)
+_sig("ntt_server_stats", _st, _vp, ctypes.c_int, ctypes.POINTER(ServerStats))
+_sig("ntt_server_destroy", _st, _vp)
+
+
+def _host_ptr(a) -> int:
+    """Address of a C-contiguous host buffer (numpy array or CPU tensor)."""
+    if hasattr(a, "ctypes"):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("host buffers must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if getattr(a, "is_cuda", False):
+            raise ValueError("expected a host buffer")
+        return int(a.data_ptr())
+    if isinstance(a, int):
+        return a
+    raise TypeError(f"cannot take a host pointer of {type(a)!r}")
+
+
+class Server:
+    """Continuous-batching request loop.  Requests carry host buffers of
+    limbs * 2^logN uint32 words (pinned memory keeps the copies
+    asynchronous); results are written to `output` when the ticket
+    completes.  The Python object keeps every buffer of a pending request
+    alive until its ticket is waited on or polled complete."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, streams: int = 0, max_round_tiles: int = 0,
+                 cluster_ctas: int = 0):
+        o = ServerOptions(hbm_budget_bytes, streams, max_round_tiles, cluster_ctas)
+        h = _vp()
+        _check(_lib.ntt_server_create(ctypes.byref(o), ctypes.byref(h)), "ntt_server_create")
+        self._h = h
+        self._live = {}
+
+    def submit(self, op: int, logN: int, moduli: Sequence, input, output, operand=None,
+               operand_handle: int = 0) -> int:
+        m, n = _moduli_array(moduli)
+        r = Request(op, logN, n, ctypes.cast(m, ctypes.POINTER(ModulusConfig)), _host_ptr(input),
+                    _host_ptr(operand) if operand is not None else None, operand_handle,
+                    _host_ptr(output))
+        t = ctypes.c_uint64()
+        _check(_lib.ntt_server_submit(self._h, ctypes.byref(r), ctypes.byref(t)),
+               "ntt_server_submit")
+        self._live[t.value] = (input, output, operand)
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        st = _lib.ntt_server_poll(self._h, ticket)
+        if st == 12:  # NTT_ERR_NOT_READY
+            return False
+        self._live.pop(ticket, None)
+        _check(st, "ntt_server_poll")
+        return True
+
+    def wait(self, ticket: int, timeout: float = -1.0):
+        st = _lib.ntt_server_wait(self._h, ticket, timeout)
+        if st != 10:  # NTT_ERR_TIMEOUT keeps the buffers alive
+            self._live.pop(ticket, None)
+        _check(st, "ntt_server_wait")
+
+    def latency_ms(self, ticket: int) -> float:
+        return _lib.ntt_server_latency_ms(self._h, ticket)
+
+    def put(self, host) -> int:
+        h = ctypes.c_uint64()
+        words = int(host.size) if hasattr(host, "size") and not callable(host.size) else host.numel()
+        _check(_lib.ntt_server_put(self._h, _host_ptr(host), words, ctypes.byref(h)),
+               "ntt_server_put")
+        return h.value
+
+    def drop(self, handle: int):
+        _check(_lib.ntt_server_drop(self._h, handle), "ntt_server_drop")
+
+    def stats(self, reset: bool = False) -> dict:
+        s = ServerStats()
+        _check(_lib.ntt_server_stats(self._h, 1 if reset else 0, ctypes.byref(s)),
+               "ntt_server_stats")
+        return s.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.ntt_server_destroy(self._h)
+            self._h = _vp()
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -75,18 +75,25 @@ ntt_status_t acquire_tables(int logN, const ModulusConfig* mods, int count,
         const size_t N = size_t{1} << logN;
         auto slab = std::make_shared<TableSlab>();
         slab->device = dev;
-        slab->bytes = 2 * (size_t)m * N * sizeof(TwPair);
-        TwGenLimb* gdev = nullptr;
-        cudaError_t e = cudaMalloc(&slab->block, slab->bytes);
-        if (e == cudaSuccess) e = cudaMalloc(&gdev, gen.size() * sizeof(TwGenLimb));
-        if (e == cudaSuccess)
-            e = cudaMemcpy(gdev, gen.data(), gen.size() * sizeof(TwGenLimb), cudaMemcpyHostToDevice);
+        const size_t tab_bytes = 2 * (size_t)m * N * sizeof(TwPair);
+        slab->bytes = tab_bytes + gen.size() * sizeof(TwGenLimb);
+        // generation on a private non-blocking stream, synchronised alone:
+        // no device-wide synchronisation, so running batches (a serving
+        // loop's rounds) are not stalled; the generator inputs stay in the
+        // slab (no cudaFree, which would synchronise the device)
+        cudaStream_t gs = nullptr;
+        cudaError_t e = cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaMalloc(&slab->block, slab->bytes);
         TwPair* fwd = (TwPair*)slab->block;
         TwPair* inv = fwd + (size_t)m * N;
-        if (e == cudaSuccess) e = launch_twiddle_gen(fwd, gdev, m, logN, 0);
-        if (e == cudaSuccess) e = launch_twiddle_gen(inv, gdev + m, m, logN, 0);
-        if (e == cudaSuccess) e = cudaDeviceSynchronize();
-        if (gdev) cudaFree(gdev);
+        TwGenLimb* gdev = (TwGenLimb*)((char*)slab->block + tab_bytes);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(gdev, gen.data(), gen.size() * sizeof(TwGenLimb),
+                                cudaMemcpyHostToDevice, gs);
+        if (e == cudaSuccess) e = launch_twiddle_gen(fwd, gdev, m, logN, gs);
+        if (e == cudaSuccess) e = launch_twiddle_gen(inv, gdev + m, m, logN, gs);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(gs);
+        if (gs) cudaStreamDestroy(gs);
         if (e != cudaSuccess) {
             if (e == cudaErrorMemoryAllocation) {
                 cudaGetLastError();

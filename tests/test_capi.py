@@ -157,3 +157,13 @@ def test_ragged_mix_is_seeded():
         for q, g in j.moduli:
             assert (q - 1) % (2 << j.logN) == 0 and (1 << 29) < q < (1 << 30)
     assert len({tuple(j.moduli) for j in a}) > 40  # chains differ between polynomials
+
+
+def test_server_and_batch_without_device_fail_cleanly():
+    with pytest.raises(nb.NttError) as e:
+        nb.Server(hbm_budget_bytes=1 << 20)
+    assert e.value.name in ("NTT_ERR_CUDA", "NTT_ERR_OUT_OF_MEMORY")
+    with pytest.raises(nb.NttError) as e:
+        nb.Server(streams=-1)
+    assert e.value.name == "NTT_ERR_INVALID_ARGUMENT"
+    assert nb.tables_device_bytes() == 0

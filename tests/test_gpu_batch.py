@@ -189,7 +189,8 @@ def test_tables_shared_and_trimmed(torch_cuda, nb, mixes):
     b = nb.Batch([(j.op, j.logN, j.moduli, x, None) for j, x in zip(jobs, data)])
     held = nb.tables_device_bytes()
     distinct = len({m for j in jobs for m in j.moduli})
-    assert held - base == distinct * (1 << 13) * 16
+    # two tables of 2^13 (w, w') pairs per modulus + its 2 x 28-byte generator inputs
+    assert held - base == distinct * ((1 << 13) * 16 + 56)
     nb.tables_trim()
     assert nb.tables_device_bytes() == held  # still used by the batch
     b.close()
