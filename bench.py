@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-steps", type=int, default=20)
     ap.add_argument("--plain-steps", type=int, default=5)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=20000)
+    ap.add_argument("--serve-loads", type=str, default="0.5,0.8,0.95")
     return ap.parse_args()
 
 
@@ -325,6 +328,8 @@ def run_ours(args):
         out["batched"] = bench_batched(args, torch, nb, stream)
         out["gpu_launches_batched"] = 2 * (args.batched_steps + args.plain_steps *
                                            out["batched"]["polynomials"])
+    if not args.no_serve:
+        out["serve"] = bench_serve(args, torch, nb)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, kind, reps, el = cpu_roundtrip_rate(args.cpu_seconds, threads)
@@ -416,6 +421,94 @@ def bench_batched(args, torch, nb, stream):
     for p in plans:
         p.close()
     return res
+
+
+SERVE = dict(seed=SEED, logn=tuple(range(12, 18)), limbs=(1, 64), bits=(30, 31),
+             ops=((0, 0.4), (1, 0.4), (2, 0.2)))
+
+
+def bench_serve(args, torch, nb):
+    """Serving stream: requests with logN uniform in 12..17, limbs uniform in
+    1..64, 30/31-bit moduli chains, 40% NTT / 40% INTT / 20% multiply, host
+    (pinned) buffers in and out.  Capacity = all requests submitted at once;
+    then Poisson arrivals at fractions of that capacity (open loop), p50/p99
+    of submit -> result-in-host-buffer.  The plain per-call form is the same
+    server with batching off (one request per launch, one stream)."""
+    from ntt_b200 import mixes
+    jobs = mixes.ragged_mix(count=args.serve_requests, **SERVE)
+    # preload every modulus the stream names (tables stay resident)
+    for lg in SERVE["logn"]:
+        for b in SERVE["bits"]:
+            nb.tables_preload(lg, mixes.prime_pool(lg, b, 96))
+    # host pools: inputs < 2^29 are valid for every op and modulus; outputs of
+    # the same logN share one pinned buffer (their contents are not checked)
+    gen = torch.Generator().manual_seed(SEED)
+    pool = {lg: torch.randint(0, 1 << 29, (64, 1 << lg), dtype=torch.int32, generator=gen)
+                 .pin_memory().numpy().view(np.uint32) for lg in SERVE["logn"]}
+    sink = {lg: torch.empty((64, 1 << lg), dtype=torch.int32).pin_memory().numpy()
+                 .view(np.uint32) for lg in SERVE["logn"]}
+    limb_ntts = sum(j.limbs * (3 if j.op == nb.OP_MULTIPLY else 1) for j in jobs)
+    byts = sum(j.words * 4 * (3 if j.op == nb.OP_MULTIPLY else 2) for j in jobs)
+
+    def run(srv, rate):
+        srv.stats(reset=True)
+        rng = np.random.default_rng(SEED)
+        gaps = rng.exponential(1.0 / rate, len(jobs)) if rate else None
+        t0 = time.perf_counter()
+        t_next = t0
+        tickets = []
+        for i, j in enumerate(jobs):
+            if gaps is not None:
+                t_next += gaps[i]
+                while time.perf_counter() < t_next:
+                    pass
+            x = pool[j.logN][:j.limbs]
+            tickets.append(srv.submit(j.op, j.logN, j.moduli, x, sink[j.logN][:j.limbs],
+                                      operand=x if j.op == nb.OP_MULTIPLY else None))
+        for t in tickets:
+            srv.wait(t, 300.0)
+        st = srv.stats(reset=True)
+        return {"offered_rps": rate, "achieved_rps": len(jobs) / st["elapsed_s"],
+                "limb_ntt_per_s": st["limb_ntt_per_s"], "p50_ms": st["p50_ms"],
+                "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
+                "rounds": st["rounds"], "mean_round_requests": st["mean_round_requests"],
+                "arena_peak_bytes": st["arena_peak_bytes"], "elapsed_s": st["elapsed_s"]}
+
+    loads = [float(v) for v in args.serve_loads.split(",") if v]
+    out = {"workload": f"{len(jobs)} requests: logN uniform 12..17, limbs uniform 1..64, 30/31-bit "
+                       "chains, 40% NTT / 40% INTT / 20% multiply, pinned host buffers in and "
+                       "out; latency = submit -> result in the host buffer",
+           "limb_ntts": limb_ntts, "pcie_bytes": byts}
+    with nb.Server() as srv:  # 80 GB budget, 4 streams, rounds of up to 1024 tiles
+        # correctness spot check against the plain per-call path
+        chk = [j for j in jobs[:200] if j.limbs <= 8][:6]
+        for j in chk:
+            x = pool[j.logN][:j.limbs].copy()
+            o = np.empty_like(x)
+            srv.wait(srv.submit(j.op, j.logN, j.moduli, x, o,
+                                operand=x if j.op == nb.OP_MULTIPLY else None), 60.0)
+            p = nb.Plan(j.logN, j.moduli)
+            d = torch.from_numpy(x.view(np.int32)).cuda()
+            if j.op == nb.OP_FORWARD:
+                p.forward(d)
+            elif j.op == nb.OP_INVERSE:
+                p.inverse(d)
+            else:
+                continue  # multiply parity is covered by the tests
+            torch.cuda.synchronize()
+            if not np.array_equal(d.cpu().numpy().view(np.uint32), o):
+                raise RuntimeError("served result differs from the plain path")
+            p.close()
+        cap = run(srv, None)
+        out["batched"] = {"capacity": cap, "poisson": [run(srv, f * cap["achieved_rps"])
+                                                         for f in loads]}
+        out["budget_bytes"] = srv.stats()["budget_bytes"]
+    with nb.Server(streams=1, max_round_requests=1) as srv:
+        cap_p = run(srv, None)
+        out["plain_per_call"] = {"capacity": cap_p,
+                                 "poisson": [run(srv, 0.5 * cap_p["achieved_rps"])]}
+    out["capacity_speedup_vs_plain"] = cap["achieved_rps"] / cap_p["achieved_rps"]
+    return out
 
 
 def main():

@@ -84,6 +84,10 @@ NTT_API ntt_status_t ntt_batch_submit(const ntt_job_t* jobs, int count, ntt_stre
 /* Resident twiddle-table registry: bytes held on the current device, and a
  * release of every table no live batch or server uses. */
 NTT_API size_t ntt_tables_device_bytes(void);
+/* Generates (if missing) the tables of `count` moduli for logN on the
+ * current device and keeps them in the registry, so that a later batch or
+ * request naming them does not pay for their generation. */
+NTT_API ntt_status_t ntt_tables_preload(int logN, const ModulusConfig* moduli, int count);
 NTT_API void ntt_tables_trim(void);
 
 #ifdef __cplusplus

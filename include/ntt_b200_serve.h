@@ -32,9 +32,11 @@ typedef struct ntt_server ntt_server_t;
 
 typedef struct ntt_server_options {
     size_t hbm_budget_bytes; /* device arena; 0 = 80 GB (capped by free memory) */
-    int streams;             /* rounds in flight at once; 0 = 3 */
-    int max_round_tiles;     /* (polynomial, limb) tiles per launch; 0 = 16384 */
+    int streams;             /* rounds in flight at once; 0 = 4 */
+    int max_round_tiles;     /* (polynomial, limb) tiles per launch; 0 = 1024 */
     int cluster_ctas;        /* 0 = automatic per round (8, or 16 with logN 17) */
+    int max_round_requests;  /* requests per launch; 0 = no limit (1 with streams = 1
+                                turns batching off: one request per launch, in order) */
 } ntt_server_options_t;
 
 typedef struct ntt_request {

@@ -440,6 +440,7 @@ _sig("ntt_batch_destroy", _st, _vp)
 _sig("ntt_batch_submit", _st, ctypes.POINTER(Job), ctypes.c_int, _vp)
 _sig("ntt_tables_device_bytes", ctypes.c_size_t)
 _sig("ntt_tables_trim", None)
+_sig("ntt_tables_preload", _st, ctypes.c_int, ctypes.POINTER(ModulusConfig), ctypes.c_int)
 
 
 def _job_array(jobs: Sequence) -> tuple:
@@ -510,6 +511,12 @@ def tables_trim():
     _lib.ntt_tables_trim()
 
 
+def tables_preload(logN: int, moduli: Sequence):
+    """Generate and keep the device tables of these moduli for logN."""
+    m, n = _moduli_array(moduli)
+    _check(_lib.ntt_tables_preload(logN, m, n), "ntt_tables_preload")
+
+
 # ---------------------------------------------------------------------------
 # serving loop (include/ntt_b200_serve.h)
 # ---------------------------------------------------------------------------
@@ -523,7 +530,8 @@ class Request(ctypes.Structure):
 
 class ServerOptions(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("streams", ctypes.c_int),
-                ("max_round_tiles", ctypes.c_int), ("cluster_ctas", ctypes.c_int)]
+                ("max_round_tiles", ctypes.c_int), ("cluster_ctas", ctypes.c_int),
+                ("max_round_requests", ctypes.c_int)]
 
 
 class ServerStats(ctypes.Structure):
@@ -574,8 +582,9 @@ class Server:
     alive until its ticket is waited on or polled complete."""
 
     def __init__(self, hbm_budget_bytes: int = 0, streams: int = 0, max_round_tiles: int = 0,
-                 cluster_ctas: int = 0):
-        o = ServerOptions(hbm_budget_bytes, streams, max_round_tiles, cluster_ctas)
+                 cluster_ctas: int = 0, max_round_requests: int = 0):
+        o = ServerOptions(hbm_budget_bytes, streams, max_round_tiles, cluster_ctas,
+                          max_round_requests)
         h = _vp()
         _check(_lib.ntt_server_create(ctypes.byref(o), ctypes.byref(h)), "ntt_server_create")
         self._h = h

@@ -453,4 +453,13 @@ size_t ntt_tables_device_bytes(void) {
 
 void ntt_tables_trim(void) { tables_trim(); }
 
+ntt_status_t ntt_tables_preload(int logN, const ModulusConfig* moduli, int count) {
+    if (count < 1 || !moduli) return fail(NTT_ERR_INVALID_ARGUMENT, "need at least one modulus");
+    if (logN < NTT_BATCH_MIN_LOGN || logN > NTT_BATCH_MAX_LOGN)
+        return fail(NTT_ERR_UNSUPPORTED, "logN %d outside [%d, %d]", logN, NTT_BATCH_MIN_LOGN,
+                    NTT_BATCH_MAX_LOGN);
+    std::vector<TableRef> refs;
+    return acquire_tables(logN, moduli, count, refs);
+}
+
 }  // extern "C"

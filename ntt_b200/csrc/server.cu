@@ -270,6 +270,8 @@ void scheduler_main(ntt_server* S) {
         while (!S->pending.empty()) {
             ReqP r = S->pending.front();
             if (!take.empty() && tiles + (size_t)r->limbs > (size_t)S->opt.max_round_tiles) break;
+            if (S->opt.max_round_requests && take.size() >= (size_t)S->opt.max_round_requests)
+                break;
             const size_t od = S->arena.alloc(r->bytes);
             if (od == kNone) break;
             size_t oo = kNone;
@@ -343,12 +345,14 @@ ntt_status_t ntt_server_create(const ntt_server_options_t* opts, ntt_server_t** 
     *out = nullptr;
     ntt_server_options_t o{};
     if (opts) o = *opts;
-    if (o.streams < 0 || o.max_round_tiles < 0 || (o.cluster_ctas != 0 && o.cluster_ctas != 8 &&
-                                                   o.cluster_ctas != 16))
+    if (o.streams < 0 || o.max_round_tiles < 0 || o.max_round_requests < 0 ||
+        (o.cluster_ctas != 0 && o.cluster_ctas != 8 && o.cluster_ctas != 16))
         return fail(NTT_ERR_INVALID_ARGUMENT, "bad server options");
     if (!o.hbm_budget_bytes) o.hbm_budget_bytes = size_t{80} << 30;
-    if (!o.streams) o.streams = 3;
-    if (!o.max_round_tiles) o.max_round_tiles = 16384;
+    // defaults from a sweep on B200 at saturating load: the PCIe copies
+    // pipeline once rounds hold ~1k tiles and 3-4 rounds are in flight
+    if (!o.streams) o.streams = 4;
+    if (!o.max_round_tiles) o.max_round_tiles = 1024;
     auto S = std::make_unique<ntt_server>();
     if (cudaGetDevice(&S->device) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaGetDevice");
     size_t free_b = 0, total_b = 0;
