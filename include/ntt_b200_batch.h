@@ -81,6 +81,25 @@ NTT_API ntt_status_t ntt_batch_destroy(ntt_batch_t* batch);
 /* create + run + wait + destroy. */
 NTT_API ntt_status_t ntt_batch_submit(const ntt_job_t* jobs, int count, ntt_stream_t stream);
 
+/* Allocation-free variant of ntt_batch_submit (no reference counterpart:
+ * the reference allocates nothing per call but also batches nothing).
+ * For callers that must not allocate device memory while they run -- code
+ * living inside a fixed, pre-sized memory reservation, or a latency-critical
+ * loop where cudaMalloc / cudaFree would synchronise the device -- it runs
+ * the batch kernel with its descriptors in a fixed 464 KiB scratch array
+ * compiled into the library instead of allocated buffers.
+ * Limits: at most NTT_NOALLOC_MAX_TILES (polynomial, limb) tiles per call
+ * (NTT_ERR_UNSUPPORTED beyond); every modulus's tables must already be
+ * resident (ntt_tables_preload beforehand, else NTT_ERR_NOT_READY).  The
+ * scratch holds one call, so calls must not overlap on the device: issue
+ * them on one stream or wait between them -- overlapping calls race.  The
+ * scratch's group counter must be zero at kernel start; each call zeroes it
+ * on `stream` itself.  The first call on a device looks up the scratch's
+ * address (one-time set-up); make it before any stream capture.  Does not
+ * wait for the kernel. */
+#define NTT_NOALLOC_MAX_TILES 4096
+NTT_API ntt_status_t ntt_batch_run_noalloc(const ntt_job_t* jobs, int count, ntt_stream_t stream);
+
 /* Resident twiddle-table registry: bytes held on the current device, and a
  * release of every table no live batch or server uses. */
 NTT_API size_t ntt_tables_device_bytes(void);

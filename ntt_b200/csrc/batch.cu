@@ -112,6 +112,17 @@ ntt_status_t acquire_tables(int logN, const ModulusConfig* mods, int count,
     return NTT_OK;
 }
 
+bool find_resident_table(int dev, int logN, ModulusConfig m, const TwPair** fwd,
+                         const TwPair** inv, uint32_t* nqinv) {
+    std::lock_guard<std::mutex> lk(g_tab_mu);
+    auto it = g_tables.find({dev, logN, m.qi, m.primitive_root});
+    if (it == g_tables.end()) return false;
+    *fwd = it->second.fwd;
+    *inv = it->second.inv;
+    *nqinv = it->second.nqinv;
+    return true;
+}
+
 size_t tables_device_bytes(int dev) {
     std::lock_guard<std::mutex> lk(g_tab_mu);
     std::set<const TableSlab*> seen;

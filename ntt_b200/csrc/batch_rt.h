@@ -34,6 +34,10 @@ struct TableRef {
 ntt_status_t acquire_tables(int logN, const ModulusConfig* mods, int count,
                             std::vector<TableRef>& out);
 size_t tables_device_bytes(int device);
+// Registry lookup only (never generates or allocates): false when the
+// tables of (logN, m) are not resident on `device`.
+bool find_resident_table(int device, int logN, ModulusConfig m, const TwPair** fwd,
+                         const TwPair** inv, uint32_t* nqinv);
 void tables_trim();
 
 const void* batch_kernel_fn(int cluster_ctas, bool mul);
