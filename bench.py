@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-steps", type=int, default=20)
     ap.add_argument("--plain-steps", type=int, default=5)
+    ap.add_argument("--no-multiply", action="store_true")
+    ap.add_argument("--multiply-steps", type=int, default=10)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=20000)
     ap.add_argument("--serve-loads", type=str, default="0.5,0.8,0.95")
@@ -328,6 +330,8 @@ def run_ours(args):
         out["batched"] = bench_batched(args, torch, nb, stream)
         out["gpu_launches_batched"] = 2 * (args.batched_steps + args.plain_steps *
                                            out["batched"]["polynomials"])
+    if not args.no_multiply:
+        out["fused_multiply"] = bench_multiply(args, torch, nb, stream)
     if not args.no_serve:
         out["serve"] = bench_serve(args, torch, nb)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -420,6 +424,70 @@ def bench_batched(args, torch, nb, stream):
     bi.close()
     for p in plans:
         p.close()
+    return res
+
+
+def bench_multiply(args, torch, nb, stream):
+    """Fused negacyclic multiply: 128 pairs of 2^16 x 24-limb polynomials
+    (24 ascending 30-bit primes q == 1 mod 2^17 above 2^29.5), uniform [0, q)
+    coefficients; c = a * b into b's buffer.  Fused: one persistent launch of
+    multiply tiles (NTT(a), NTT(b), pointwise Montgomery product, INTT per
+    limb, a read once, b read and overwritten once).  Unfused: the plain
+    calls forward_many(a), forward_many(b), pointwise_mul, inverse_many(b)
+    (4 launches; a is overwritten by its spectrum, which favours it)."""
+    from ntt_b200 import mixes
+    logN, limbs, pairs = 16, 24, 128
+    mods = list(mixes.prime_pool(logN, 30, limbs))
+    job = mixes.MixJob(nb.OP_MULTIPLY, logN, mods)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    a = torch.stack([mixes.uniform_device(torch, job, g) for _ in range(pairs)])
+    b = torch.stack([mixes.uniform_device(torch, job, g) for _ in range(pairs)])
+    sh = stream.cuda_stream
+    p = nb.Plan(logN, mods)
+    fused = nb.Batch([(nb.OP_MULTIPLY, logN, mods, b[i], a[i]) for i in range(pairs)])
+    # consistency of the two forms on this workload (parity is the tests' job)
+    b0 = b.clone()
+    ta, tb = a.clone(), b.clone()
+    with torch.cuda.stream(stream):
+        fused.run(sh)
+        p.forward_many(ta, pairs, 0, sh)
+        p.forward_many(tb, pairs, 0, sh)
+        p.pointwise_mul(tb, ta, tb, pairs, 0, sh)
+        p.inverse_many(tb, pairs, 0, sh)
+    stream.synchronize()
+    if not torch.equal(b, tb):
+        raise RuntimeError("fused and unfused multiply differ")
+    del b0
+
+    def unfused():
+        p.forward_many(ta, pairs, 0, sh)
+        p.forward_many(tb, pairs, 0, sh)
+        p.pointwise_mul(tb, ta, tb, pairs, 0, sh)
+        p.inverse_many(tb, pairs, 0, sh)
+
+    w = 3
+    fused_ms = device_time(torch, stream, lambda: fused.run(sh), args.multiply_steps, w)
+    unfused_ms = device_time(torch, stream, unfused, args.multiply_steps, w)
+    products = pairs * limbs
+    words = pairs * limbs << logN
+    res = {
+        "workload": f"{pairs} pairs of 2^{logN} x {limbs}-limb polynomials, 30-bit primes, "
+                    "c = a*b negacyclic per limb into b",
+        "value": products / (fused_ms / 1000.0), "unit": "limb-products/s",
+        "limb_ntt_per_s": 3 * products / (fused_ms / 1000.0),
+        "ms_per_step": fused_ms, "launches_per_step": 1,
+        "algorithmic_bytes": 12 * words,
+        "achieved_gbs": 12 * words / (fused_ms / 1000.0) / 1e9,
+        "unfused": {"value": products / (unfused_ms / 1000.0), "ms_per_step": unfused_ms,
+                    "launches_per_step": 4, "algorithmic_bytes": 36 * words},
+        "speedup_vs_unfused": unfused_ms / fused_ms,
+        "kernel": {"cluster_ctas": fused.info.cluster_ctas, "clusters": fused.info.clusters,
+                   "smem_bytes": fused.info.smem_bytes},
+        "steps": args.multiply_steps, "warmup": w,
+    }
+    fused.close()
+    p.close()
     return res
 
 

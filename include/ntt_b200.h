@@ -158,6 +158,14 @@ NTT_API ntt_status_t ntt_forward_many(const ntt_plan_t* plan, uint32_t* a_dev, s
                               size_t poly_stride, ntt_stream_t stream);
 NTT_API ntt_status_t ntt_inverse_many(const ntt_plan_t* plan, uint32_t* a_dev, size_t polys,
                               size_t poly_stride, ntt_stream_t stream);
+/* c = a (.) b: pointwise Montgomery product of two forward outputs (x*2^32
+ * domain) per limb modulus, giving the spectrum of the negacyclic product
+ * for ntt_inverse.  Over `polys` polynomials (poly_stride words apart, 0 =
+ * packed); 16-byte aligned; c may alias a or b.  No reference counterpart
+ * (the middle step of an unfused negacyclic multiply). */
+NTT_API ntt_status_t ntt_pointwise_mul(const ntt_plan_t* plan, uint32_t* c_dev,
+                                       const uint32_t* a_dev, const uint32_t* b_dev, size_t polys,
+                                       size_t poly_stride, ntt_stream_t stream);
 
 /* ---- drop-in launchers (src/v04_montgomery.cu:603-658) -----------------
  * Same arguments and domain contract as launch_ntt<LC> / launch_intt<LC>:

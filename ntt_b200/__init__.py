@@ -145,6 +145,7 @@ _sig("ntt_forward", _st, _vp, _vp, _vp)
 _sig("ntt_inverse", _st, _vp, _vp, _vp)
 _sig("ntt_forward_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_inverse_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
+_sig("ntt_pointwise_mul", _st, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_launch_ntt", _st, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_int,
      ctypes.POINTER(PhaseConfig), ctypes.POINTER(PhaseConfig))
 _sig("ntt_launch_intt", _st, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_int,
@@ -334,6 +335,11 @@ class Plan:
     def inverse_many(self, a, polys: int, poly_stride: int = 0, stream=None):
         _check(_lib.ntt_inverse_many(self._h, _ptr(a), polys, poly_stride, _stream(stream)),
                "ntt_inverse_many")
+
+    def pointwise_mul(self, c, a, b, polys: int = 1, poly_stride: int = 0, stream=None):
+        """c = a (.) b: Montgomery product of two forward outputs per limb."""
+        _check(_lib.ntt_pointwise_mul(self._h, _ptr(c), _ptr(a), _ptr(b), polys, poly_stride,
+                                      _stream(stream)), "ntt_pointwise_mul")
 
 
 # ---------------------------------------------------------------------------

@@ -17,6 +17,7 @@
 #include "configs.h"
 #include "fused_kernel.cuh"
 #include "host_math.h"
+#include "pointwise.h"
 #include "runtime.h"
 #include "small.h"
 #include "twiddle.h"
@@ -598,6 +599,24 @@ ntt_status_t ntt_forward_many(const ntt_plan_t* p, uint32_t* a, size_t polys, si
 ntt_status_t ntt_inverse_many(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
                               ntt_stream_t s) {
     return plan_run(p, a, polys, stride, false, s);
+}
+
+ntt_status_t ntt_pointwise_mul(const ntt_plan_t* p, uint32_t* c, const uint32_t* a,
+                               const uint32_t* b, size_t polys, size_t stride, ntt_stream_t s) {
+    if (!p || !c || !a || !b) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (p->logN < 2) return fail(NTT_ERR_UNSUPPORTED, "pointwise product needs logN >= 2");
+    if (stride == 0) stride = (size_t)p->limbs << p->logN;
+    if (((uintptr_t)c | (uintptr_t)a | (uintptr_t)b) % 16 || (polys > 1 && stride % 4))
+        return fail(NTT_ERR_MISALIGNED, "pointwise operands must be 16-byte aligned");
+    int dev = 0;
+    NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev != p->device)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "plan was created on device %d, current is %d",
+                    p->device, dev);
+    NTT_CUDA_TRY(launch_pointwise(c, a, b, p->q, p->limbs, p->logN, polys, stride,
+                                  (cudaStream_t)s),
+                 "pointwise launch");
+    return NTT_OK;
 }
 
 }  // extern "C"

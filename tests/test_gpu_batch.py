@@ -211,3 +211,56 @@ def test_batch_errors(torch_cuda, nb, mixes):
     with pytest.raises(nb.NttError) as e:
         nb.Batch([(nb.OP_FORWARD, 17, mixes.prime_pool(17, 30, 1), x, None)], cluster_ctas=8)
     assert e.value.name == "NTT_ERR_UNSUPPORTED"
+
+
+@pytest.mark.parametrize("logN", [15, 16])
+def test_config4_fused_vs_unfused_multiply(torch_cuda, nb, mixes, logN):
+    """Fused negacyclic multiply (one persistent launch) against the unfused
+    plain calls (forward, forward, ntt_pointwise_mul, inverse) at the
+    multiply configuration's shape: N = 2^15 / 2^16, 24 limbs of 30-bit
+    primes; plus 64 sampled (pair, limb, coefficient) schoolbook checks."""
+    torch = torch_cuda
+    pairs, limbs = 3, 24
+    mods = list(mixes.prime_pool(logN, 30, 24))
+    job = mixes.MixJob(nb.OP_MULTIPLY, logN, mods)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(40 + logN)
+    a = torch.stack([mixes.uniform_device(torch, job, g) for _ in range(pairs)])
+    b = torch.stack([mixes.uniform_device(torch, job, g) for _ in range(pairs)])
+    a_h, b_h = host(a).copy(), host(b).copy()
+    # unfused plain calls on copies
+    p = nb.Plan(logN, mods)
+    ta, tb = a.clone(), b.clone()
+    p.forward_many(ta, pairs)
+    p.forward_many(tb, pairs)
+    p.pointwise_mul(tb, ta, tb, pairs)
+    p.inverse_many(tb, pairs)
+    # fused: one batch of multiply tiles
+    with nb.Batch([(nb.OP_MULTIPLY, logN, mods, b[i], a[i]) for i in range(pairs)]) as bt:
+        bt.run()
+    torch.cuda.synchronize()
+    assert torch.equal(b, tb)
+    assert torch.equal(a, torch.from_numpy(a_h.view(np.int32)).cuda())  # operand untouched
+    c = host(b)
+    rng = np.random.default_rng(logN)
+    for _ in range(64):
+        i, l, k = int(rng.integers(pairs)), int(rng.integers(limbs)), int(rng.integers(1 << logN))
+        assert int(c[i, l, k]) == O.negacyclic_coeff(a_h[i, l], b_h[i, l], logN, mods[l][0], k)
+    p.close()
+
+
+def test_pointwise_mul_matches_numpy(torch_cuda, nb, mixes):
+    torch = torch_cuda
+    mods = list(mixes.prime_pool(13, 31, 5))
+    job = mixes.MixJob(nb.OP_FORWARD, 13, mods)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    x = torch.stack([mixes.uniform_device(torch, job, g) for _ in range(2)])
+    y = torch.stack([mixes.uniform_device(torch, job, g) for _ in range(2)])
+    z = torch.empty_like(x)
+    p = nb.Plan(13, mods)
+    p.pointwise_mul(z, x, y, 2)
+    torch.cuda.synchronize()
+    for i in range(2):
+        assert np.array_equal(host(z)[i], mont_pointwise(host(x)[i], host(y)[i], mods))
+    p.close()
