@@ -115,23 +115,22 @@ void effective_triples(const FusedConfig* c, int logN, TransformConfig* t) {
 static std::mutex g_attr_mu;
 static std::set<std::pair<int, const void*>> g_attr_done;
 
-static uint32_t smem_of(const FusedConfig* c, const void* fn) {
-    return (fn == c->fwd_direct || fn == c->inv_direct) ? c->smem_bytes_direct : c->smem_bytes;
+static uint32_t smem_of(const FusedConfig* c, int schedule) {
+    return schedule == NTT_SCHEDULE_STAGED ? c->smem_bytes : c->smem_bytes_direct;
 }
 
-static const void* kernel_of(const FusedConfig* c, bool fwd, int schedule) {
-    if (schedule == NTT_SCHEDULE_STAGED) return fwd ? c->fwd : c->inv;
-    return fwd ? c->fwd_direct : c->inv_direct;
+static const void* kernel_of(const FusedConfig* c, bool fwd, int schedule, bool lazy2) {
+    return c->kernel(schedule == NTT_SCHEDULE_STAGED, fwd, lazy2);
 }
 
-ntt_status_t prepare_function(const FusedConfig* c, const void* fn) {
+ntt_status_t prepare_function(const FusedConfig* c, const void* fn, int schedule) {
     int dev = 0;
     NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
     std::lock_guard<std::mutex> lk(g_attr_mu);
     if (g_attr_done.count({dev, fn})) return NTT_OK;
-    if (smem_of(c, fn) > 48 * 1024)
+    if (smem_of(c, schedule) > 48 * 1024)
         NTT_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem_of(c, fn)),
+                                          (int)smem_of(c, schedule)),
                      "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
     if ((1 << c->clog) > 8)
         NTT_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
@@ -144,7 +143,7 @@ ntt_status_t prepare_function(const FusedConfig* c, const void* fn) {
 static std::mutex g_occ_mu;
 static std::map<std::pair<int, const void*>, int> g_occ;
 
-static int resident_clusters(const FusedConfig* c, const void* fn) {
+static int resident_clusters(const FusedConfig* c, const void* fn, int schedule) {
     int dev = 0;
     cudaGetDevice(&dev);
     {
@@ -158,7 +157,7 @@ static int resident_clusters(const FusedConfig* c, const void* fn) {
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(C * 1024, 1, 1);
         lc.blockDim = dim3((unsigned)c->threads, 1, 1);
-        lc.dynamicSmemBytes = smem_of(c, fn);
+        lc.dynamicSmemBytes = smem_of(c, schedule);
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = C;
@@ -170,7 +169,7 @@ static int resident_clusters(const FusedConfig* c, const void* fn) {
     } else {
         int per_sm = 0, sms = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, c->threads,
-                                                          smem_of(c, fn)) == cudaSuccess &&
+                                                          smem_of(c, schedule)) == cudaSuccess &&
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
             n = per_sm * sms;
     }
@@ -182,9 +181,9 @@ static int resident_clusters(const FusedConfig* c, const void* fn) {
 }
 
 int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule) {
-    const void* fn = kernel_of(c, fwd, schedule);
-    if (prepare_function(c, fn) != NTT_OK) return -1;
-    return resident_clusters(c, fn);
+    const void* fn = kernel_of(c, fwd, schedule, false);
+    if (prepare_function(c, fn, schedule) != NTT_OK) return -1;
+    return resident_clusters(c, fn, schedule);
 }
 
 // NTT_SCHEDULE_DIRECT: one limb per cluster, input straight from global
@@ -192,15 +191,15 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule) {
 // wave of resident clusters, each running a contiguous chunk of limb-major
 // jobs with the next input slab bulk-copied ahead.
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
-                          int schedule) {
+                          int schedule, bool lazy2) {
     if (a.jobs == 0) return NTT_OK;
-    const void* fn = kernel_of(c, fwd, schedule);
-    ntt_status_t st = prepare_function(c, fn);
+    const void* fn = kernel_of(c, fwd, schedule, lazy2);
+    ntt_status_t st = prepare_function(c, fn, schedule);
     if (st != NTT_OK) return st;
     const unsigned C = 1u << c->clog;
     uint32_t per = 1;
     if (schedule == NTT_SCHEDULE_STAGED) {
-        const uint32_t resident = (uint32_t)resident_clusters(c, fn);
+        const uint32_t resident = (uint32_t)resident_clusters(c, fn, schedule);
         per = (a.jobs + resident - 1) / resident;
     }
     const uint32_t clusters = (a.jobs + per - 1) / per;
@@ -209,7 +208,7 @@ ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cu
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3(C * clusters, 1, 1);
     lc.blockDim = dim3((unsigned)c->threads, 1, 1);
-    lc.dynamicSmemBytes = smem_of(c, fn);
+    lc.dynamicSmemBytes = smem_of(c, schedule);
     lc.stream = s;
     cudaLaunchAttribute attr[1];
     if (C > 1) {
@@ -246,6 +245,7 @@ struct ntt_plan {
     TransformConfig effective{};
     int tuned = 0;
     int schedule = NTT_SCHEDULE_DIRECT;
+    bool lazy2 = false;  // a modulus >= 2^30: every limb uses the [0, 2q) discipline
 };
 
 namespace nttb {
@@ -423,6 +423,7 @@ ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int limbs,
     p->logN = logN;
     p->limbs = limbs;
     p->moduli.assign(moduli, moduli + limbs);
+    for (int l = 0; l < limbs; ++l) p->lazy2 |= moduli[l].qi >= (1u << 30);
     cudaError_t e = cudaGetDevice(&p->device);
     const size_t tw_bytes = (size_t)limbs * N * sizeof(TwPair);
     const size_t q_bytes = ((size_t)limbs * 4 + 255) & ~(size_t)255;
@@ -545,7 +546,7 @@ namespace nttb {
 
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
-                           cudaStream_t s, uint32_t* status, int schedule) {
+                           cudaStream_t s, uint32_t* status, int schedule, bool lazy2) {
     if (polys == 0) return NTT_OK;
     if (!a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL data pointer");
     // the fused kernels move 16-byte vectors; the small-size kernel words
@@ -561,7 +562,7 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
     if (cfg) {
         FusedArgs fa{a,  tw, q, (uint32_t)limbs, (uint32_t)polys, (uint32_t)jobs, 1u,
                      (unsigned long long)stride, status};
-        return launch_fused(cfg, fwd, fa, s, schedule);
+        return launch_fused(cfg, fwd, fa, s, schedule, lazy2);
     }
     SmallArgs sa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride, logN};
     NTT_CUDA_TRY(launch_small(sa, fwd, s), "small NTT launch");
@@ -579,7 +580,7 @@ static ntt_status_t plan_run(const ntt_plan_t* p, uint32_t* a, size_t polys, siz
     if (stride == 0) stride = (size_t)p->limbs << p->logN;
     return run_transform(p->logN, fwd ? p->cfg_fwd : p->cfg_inv, fwd ? p->fwd : p->inv, p->q,
                          p->limbs, a, polys, stride, fwd, (cudaStream_t)s, p->status,
-                         p->schedule);
+                         p->schedule, p->lazy2);
 }
 
 }  // namespace nttb
@@ -640,7 +641,11 @@ struct ShimKey {
     }
 };
 std::mutex g_shim_mu;
-std::map<ShimKey, TwPair*> g_shim;
+struct ShimTable {
+    TwPair* table;
+    bool lazy2;  // some modulus >= 2^30
+};
+std::map<ShimKey, ShimTable> g_shim;
 
 ntt_status_t shim_run(uint32_t* A, const uint32_t* tw, const uint32_t* moduli, const uint32_t* qinv,
                       const uint32_t* aux, size_t limbs, int logN, const PhaseConfig* ph1,
@@ -656,13 +661,21 @@ ntt_status_t shim_run(uint32_t* A, const uint32_t* tw, const uint32_t* moduli, c
     NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
     ShimKey k{dev, tw, moduli, qinv, aux, limbs, logN, inverse ? 1 : 0};
     TwPair* table = nullptr;
+    bool lazy2 = false;
     {
         std::lock_guard<std::mutex> lk(g_shim_mu);
         auto it = g_shim.find(k);
-        if (it != g_shim.end()) table = it->second;
+        if (it != g_shim.end()) {
+            table = it->second.table;
+            lazy2 = it->second.lazy2;
+        }
     }
     if (!table) {
         const size_t N = size_t{1} << logN;
+        std::vector<uint32_t> qh(limbs);
+        NTT_CUDA_TRY(cudaMemcpy(qh.data(), moduli, limbs * 4, cudaMemcpyDeviceToHost),
+                     "moduli read");
+        for (uint32_t q : qh) lazy2 |= q >= (1u << 30);
         NTT_CUDA_TRY(cudaMalloc(&table, limbs * N * sizeof(TwPair)), "cudaMalloc(shim table)");
         cudaError_t e = launch_twiddle_import(table, tw, moduli, qinv, aux, (int)limbs, logN,
                                               inverse ? 1 : 0, 0);
@@ -671,10 +684,10 @@ ntt_status_t shim_run(uint32_t* A, const uint32_t* tw, const uint32_t* moduli, c
             return cuda_fail(e, "twiddle import");
         }
         std::lock_guard<std::mutex> lk(g_shim_mu);
-        auto ins = g_shim.insert({k, table});
+        auto ins = g_shim.insert({k, ShimTable{table, lazy2}});
         if (!ins.second) {  // another thread won the race
             cudaFree(table);
-            table = ins.first->second;
+            table = ins.first->second.table;
         }
     }
     const FusedConfig* cfg = nullptr;
@@ -686,7 +699,7 @@ ntt_status_t shim_run(uint32_t* A, const uint32_t* tw, const uint32_t* moduli, c
         if (!cfg) cfg = default_config(logN, !inverse);
     }
     return run_transform(logN, cfg, table, moduli, (int)limbs, A, 1, limbs << logN, !inverse, 0,
-                         nullptr, NTT_SCHEDULE_DIRECT);
+                         nullptr, NTT_SCHEDULE_DIRECT, lazy2);
 }
 }  // namespace
 
@@ -710,7 +723,7 @@ void ntt_shim_cache_clear(void) {
         int cur = 0;
         cudaGetDevice(&cur);
         if (cur != kv.first.dev) cudaSetDevice(kv.first.dev);
-        cudaFree(kv.second);
+        cudaFree(kv.second.table);
         if (cur != kv.first.dev) cudaSetDevice(cur);
     }
     g_shim.clear();

@@ -16,12 +16,12 @@
 #define NTTB_CFG_N11(X) X(11, 0, 6, 5, 1, 5)
 #define NTTB_CFG_N12(X) X(12, 0, 7, 5, 3, 5) X(12, 0, 6, 4, 3, 3)
 #define NTTB_CFG_N13(X) X(13, 0, 8, 5, 3, 5)
-#define NTTB_CFG_N14(X) X(14, 0, 9, 5, 4, 5) X(14, 1, 9, 5, 4, 5)
-#define NTTB_CFG_N15(X) X(15, 1, 10, 5, 5, 5) X(15, 2, 8, 5, 3, 4)
+#define NTTB_CFG_N14(X) X(14, 0, 9, 5, 4, 5) X(14, 1, 9, 5, 4, 5) X(14, 1, 6, 6, 6, 4)
+#define NTTB_CFG_N15(X) X(15, 1, 10, 5, 5, 5) X(15, 2, 8, 5, 3, 4) X(15, 2, 6, 6, 6, 5)
 #define NTTB_CFG_N16(X) \
     X(16, 3, 8, 5, 3, 4) X(16, 3, 7, 5, 3, 5) X(16, 2, 8, 5, 3, 4) X(16, 4, 8, 5, 3, 4) \
-    X(16, 3, 8, 4, 4, 4)
-#define NTTB_CFG_N17(X) X(17, 3, 8, 5, 3, 5) X(17, 4, 8, 5, 3, 5)
+    X(16, 3, 8, 4, 4, 4) X(16, 3, 6, 6, 6, 5) X(16, 4, 6, 6, 6, 4)
+#define NTTB_CFG_N17(X) X(17, 3, 8, 5, 3, 5) X(17, 4, 8, 5, 3, 5) X(17, 4, 6, 6, 6, 5)
 
 #define NTTB_CFG_ALL(X)                                                                      \
     NTTB_CFG_N10(X) NTTB_CFG_N11(X) NTTB_CFG_N12(X) NTTB_CFG_N13(X) NTTB_CFG_N14(X)      \
@@ -36,10 +36,11 @@ struct FusedConfig {
     int threads;
     uint32_t smem_bytes;         // staged kernels (work + stage buffer + mbarrier)
     uint32_t smem_bytes_direct;  // direct kernels (work buffer)
-    const void* fwd;             // fused_kernel<G, true,  true>  (staged)
-    const void* inv;             // fused_kernel<G, false, true>
-    const void* fwd_direct;      // fused_kernel<G, true,  false> (direct)
-    const void* inv_direct;      // fused_kernel<G, false, false>
+    // fused_kernel<G, Fwd, Staged, Arith>: [staged][fwd][lazy2]
+    const void* kern[2][2][2];
+    const void* kernel(bool staged, bool fwd, bool lazy2) const {
+        return kern[staged ? 1 : 0][fwd ? 1 : 0][lazy2 ? 1 : 0];
+    }
 };
 
 // All compiled configurations (registry.cu); count via fused_config_count().

@@ -250,7 +250,10 @@ __device__ __forceinline__ void fused_inverse_body(Ctx& ctx, Pre&& prefetch) {
 // [j0, j1).  Staged: the CTA's input slab is bulk-copied into the stage
 // buffer one job ahead (mbarrier-tracked, bounded waits); otherwise the
 // first pass loads straight from global memory.  grid.x = C * clusters.
-template <class G, bool Fwd, bool Staged>
+// Arith: the range discipline of every limb of the launch (Lazy4 needs all
+// moduli below 2^30; Lazy2 takes any below 2^31), fixed per kernel so that
+// one path's registers fit the launch bounds.
+template <class G, bool Fwd, bool Staged, class Arith>
 __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedArgs a) {
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t rank = (G::C > 1) ? cluster_rank() : 0u;
@@ -288,13 +291,8 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedA
             if constexpr (Staged)
                 if (job + 1 < j1) issue_slab<G, Fwd>(a, job + 1, rank, stage_sa, mbar_sa);
         };
-        if (ctx.q < (1u << 30)) {
-            if constexpr (Fwd) fused_forward_body<G, Lazy4>(ctx, prefetch);
-            else fused_inverse_body<G, Lazy4>(ctx, prefetch);
-        } else {
-            if constexpr (Fwd) fused_forward_body<G, Lazy2>(ctx, prefetch);
-            else fused_inverse_body<G, Lazy2>(ctx, prefetch);
-        }
+        if constexpr (Fwd) fused_forward_body<G, Arith>(ctx, prefetch);
+        else fused_inverse_body<G, Arith>(ctx, prefetch);
         __syncthreads();  // the work buffer is rewritten by the next job
     }
 }

@@ -97,11 +97,11 @@ def search(MB, patterns):
     cands += [(a1, c1, a2, c2) for a1 in range(MB) for c1 in cs
               for a2 in range(a1 + 1, MB) for c2 in cs]
     for lay in cands:
-        deg = max(conflicts(p, lay) * w for p, w in patterns)
-        key = (deg, phys(top, *lay) + 1)
+        degs = [conflicts(p, lay) * w for p, w in patterns]
+        key = (max(degs), sum(degs), phys(top, *lay) + 1)
         if best is None or key < best[0]:
             best = (key, lay)
-    (deg, size), lay = best
+    (deg, total, size), lay = best
     return lay, size
 
 

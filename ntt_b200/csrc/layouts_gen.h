@@ -30,7 +30,7 @@ struct LayoutTable<11, 0, 6, 5, 1, 5> {
 
 template <>
 struct LayoutTable<12, 0, 7, 5, 3, 5> {
-    static constexpr int XW[5] = {6, 1, 12, 0, 4159};
+    static constexpr int XW[5] = {5, 2, 9, 1, 4357};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x21eu;
     static constexpr uint32_t lanes_P2A = 0x3e0u;
@@ -39,7 +39,7 @@ struct LayoutTable<12, 0, 7, 5, 3, 5> {
 
 template <>
 struct LayoutTable<12, 0, 6, 4, 3, 3> {
-    static constexpr int XW[5] = {6, 1, 8, 4, 4219};
+    static constexpr int XW[5] = {1, 1, 6, 5, 6458};
     static constexpr uint32_t lanes_P1A = 0x3eu;
     static constexpr uint32_t lanes_P1B = 0x3eu;
     static constexpr uint32_t lanes_P2A = 0x1c6u;
@@ -66,7 +66,7 @@ struct LayoutTable<14, 0, 9, 5, 4, 5> {
 
 template <>
 struct LayoutTable<14, 1, 9, 5, 4, 5> {
-    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
+    static constexpr int XW[5] = {5, 1, 10, 16, 8559};
     static constexpr uint32_t lanes_P1A = 0x3eu;
     static constexpr uint32_t lanes_P1B = 0x20fu;
     static constexpr uint32_t lanes_P2A = 0x3e0u;
@@ -74,8 +74,17 @@ struct LayoutTable<14, 1, 9, 5, 4, 5> {
 };
 
 template <>
+struct LayoutTable<14, 1, 6, 6, 6, 4> {
+    static constexpr int XW[5] = {6, 4, 9, 1, 8715};
+    static constexpr uint32_t lanes_P1A = 0x1fu;
+    static constexpr uint32_t lanes_P1B = 0x760u;
+    static constexpr uint32_t lanes_P2A = 0x70cu;
+    static constexpr uint32_t lanes_P2B = 0x7c0u;
+};
+
+template <>
 struct LayoutTable<15, 1, 10, 5, 5, 5> {
-    static constexpr int XW[5] = {5, 1, 14, 0, 16895};
+    static constexpr int XW[5] = {5, 1, 10, 16, 17135};
     static constexpr uint32_t lanes_P1A = 0x1fu;
     static constexpr uint32_t lanes_P1B = 0x20fu;
     static constexpr uint32_t lanes_P2A = 0x3e0u;
@@ -84,7 +93,7 @@ struct LayoutTable<15, 1, 10, 5, 5, 5> {
 
 template <>
 struct LayoutTable<15, 2, 8, 5, 3, 4> {
-    static constexpr int XW[5] = {6, 1, 8, 1, 8350};
+    static constexpr int XW[5] = {5, 1, 7, 8, 8951};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x386u;
@@ -92,8 +101,17 @@ struct LayoutTable<15, 2, 8, 5, 3, 4> {
 };
 
 template <>
+struct LayoutTable<15, 2, 6, 6, 6, 5> {
+    static constexpr int XW[5] = {5, 2, 6, 1, 8829};
+    static constexpr uint32_t lanes_P1A = 0x1fu;
+    static constexpr uint32_t lanes_P1B = 0x760u;
+    static constexpr uint32_t lanes_P2A = 0x60eu;
+    static constexpr uint32_t lanes_P2B = 0x7c0u;
+};
+
+template <>
 struct LayoutTable<16, 3, 8, 5, 3, 4> {
-    static constexpr int XW[5] = {6, 1, 9, 1, 8334};
+    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x30eu;
@@ -111,7 +129,7 @@ struct LayoutTable<16, 3, 7, 5, 3, 5> {
 
 template <>
 struct LayoutTable<16, 2, 8, 5, 3, 4> {
-    static constexpr int XW[5] = {6, 1, 9, 1, 16670};
+    static constexpr int XW[5] = {5, 1, 6, 4, 17915};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x30eu;
@@ -120,7 +138,7 @@ struct LayoutTable<16, 2, 8, 5, 3, 4> {
 
 template <>
 struct LayoutTable<16, 4, 8, 5, 3, 4> {
-    static constexpr int XW[5] = {6, 1, 9, 1, 4166};
+    static constexpr int XW[5] = {5, 1, 12, 0, 4223};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x20fu;
     static constexpr uint32_t lanes_P2A = 0x30eu;
@@ -129,11 +147,29 @@ struct LayoutTable<16, 4, 8, 5, 3, 4> {
 
 template <>
 struct LayoutTable<16, 3, 8, 4, 4, 4> {
-    static constexpr int XW[5] = {6, 1, 13, 0, 8319};
+    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
     static constexpr uint32_t lanes_P1A = 0x1fu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x10fu;
     static constexpr uint32_t lanes_P2B = 0x1f0u;
+};
+
+template <>
+struct LayoutTable<16, 3, 6, 6, 6, 5> {
+    static constexpr int XW[5] = {6, 2, 10, 1, 8453};
+    static constexpr uint32_t lanes_P1A = 0x1fu;
+    static constexpr uint32_t lanes_P1B = 0x760u;
+    static constexpr uint32_t lanes_P2A = 0x41eu;
+    static constexpr uint32_t lanes_P2B = 0x7c0u;
+};
+
+template <>
+struct LayoutTable<16, 4, 6, 6, 6, 4> {
+    static constexpr int XW[5] = {5, 1, 10, 2, 4229};
+    static constexpr uint32_t lanes_P1A = 0x1fu;
+    static constexpr uint32_t lanes_P1B = 0x7a0u;
+    static constexpr uint32_t lanes_P2A = 0x43cu;
+    static constexpr uint32_t lanes_P2B = 0x7c0u;
 };
 
 template <>
@@ -152,6 +188,15 @@ struct LayoutTable<17, 4, 8, 5, 3, 5> {
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x20fu;
     static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct LayoutTable<17, 4, 6, 6, 6, 5> {
+    static constexpr int XW[5] = {5, 1, 10, 1, 8454};
+    static constexpr uint32_t lanes_P1A = 0x1fu;
+    static constexpr uint32_t lanes_P1B = 0x760u;
+    static constexpr uint32_t lanes_P2A = 0x3eu;
+    static constexpr uint32_t lanes_P2B = 0x7c0u;
 };
 
 }  // namespace nttb

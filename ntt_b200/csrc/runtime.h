@@ -22,9 +22,10 @@ const FusedConfig* config_by_index(int idx);
 const FusedConfig* tuned_config(int logN, int limbs, bool fwd);
 // Clusters of this configuration resident at once on the current device.
 int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule);
-// One launch of a fused configuration under a schedule (NTT_SCHEDULE_*).
+// One launch of a fused configuration under a schedule (NTT_SCHEDULE_*);
+// lazy2: some modulus is >= 2^30 (the [0, 2q) range discipline for all).
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
-                          int schedule);
+                          int schedule, bool lazy2);
 ntt_status_t validate_modulus(int logN, ModulusConfig m, ModulusRuntime* rt);
 // Validates m and fills the twiddle-generation inputs of both directions
 // (entries 0/1 carry the folded Montgomery / N^{-1} R^{-1} factors).
@@ -33,6 +34,6 @@ ntt_status_t twiddle_gen_inputs(int logN, ModulusConfig m, TwGenLimb* fwd, TwGen
 // single-CTA small-size kernel).  status: optional device error word.
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
-                           cudaStream_t s, uint32_t* status, int schedule);
+                           cudaStream_t s, uint32_t* status, int schedule, bool lazy2);
 
 }  // namespace nttb

@@ -164,7 +164,7 @@ ntt_status_t ntt_autotune(int logN, int limbs, int polys, int iters, ntt_tune_re
                     for (int it = 0; it < iters && st == NTT_OK; ++it)
                         st = run_transform(logN, c, (const TwPair*)(dir ? tw_f : tw_i), qd, limbs,
                                            data, polys, (size_t)limbs << logN, dir == 1, s,
-                                           nullptr, NTT_SCHEDULE_DIRECT);
+                                           nullptr, NTT_SCHEDULE_DIRECT, false);
                     cudaEventRecord(e1, s);
                     ce = cudaEventSynchronize(e1);
                     if (ce != cudaSuccess) st = cuda_fail(ce, "autotune timing");
