@@ -166,6 +166,11 @@ NTT_API ntt_status_t ntt_inverse_many(const ntt_plan_t* plan, uint32_t* a_dev, s
 NTT_API ntt_status_t ntt_pointwise_mul(const ntt_plan_t* plan, uint32_t* c_dev,
                                        const uint32_t* a_dev, const uint32_t* b_dev, size_t polys,
                                        size_t poly_stride, ntt_stream_t stream);
+/* Diagnostic (no reference counterpart): 32-bit integer multiplies per second
+ * the current device sustains on the transforms' multiply mix (Shoup
+ * products: one multiply-high and two multiply-lows each), measured by a
+ * short kernel -- the denominator of the integer-multiply roofline. */
+NTT_API ntt_status_t ntt_measure_int_peak(double* muls_per_second);
 
 /* ---- drop-in launchers (src/v04_montgomery.cu:603-658) -----------------
  * Same arguments and domain contract as launch_ntt<LC> / launch_intt<LC>:

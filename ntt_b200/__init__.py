@@ -146,6 +146,7 @@ _sig("ntt_inverse", _st, _vp, _vp, _vp)
 _sig("ntt_forward_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_inverse_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_pointwise_mul", _st, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
+_sig("ntt_measure_int_peak", _st, ctypes.POINTER(ctypes.c_double))
 _sig("ntt_launch_ntt", _st, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_int,
      ctypes.POINTER(PhaseConfig), ctypes.POINTER(PhaseConfig))
 _sig("ntt_launch_intt", _st, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_int,
@@ -374,6 +375,13 @@ def launch_intt(A_dev, inv_twiddle_dev, moduli_dev, q_inv_dev, degree_inv_dev, l
 
 def shim_cache_clear():
     _lib.ntt_shim_cache_clear()
+
+
+def measure_int_peak() -> float:
+    """32-bit multiplies per second of the current device on the Shoup mix."""
+    v = ctypes.c_double()
+    _check(_lib.ntt_measure_int_peak(ctypes.byref(v)), "ntt_measure_int_peak")
+    return v.value
 
 
 # ---------------------------------------------------------------------------
