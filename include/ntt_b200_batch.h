@@ -16,6 +16,9 @@
  *   NTT_OP_MULTIPLY  data <- a * data  negacyclic, mod each q, normal domain
  *                    in and out: INTT(NTT(a) (.) NTT(data)) with (.) the
  *                    pointwise Montgomery product; a = operand, read only.
+ *   NTT_OP_MULTIPLY_SPECTRUM  data <- INTT(A (.) NTT(data)): the same product
+ *                    with the operand given as its spectrum A = NTT(a) (a
+ *                    forward output, e.g. kept resident), two transforms.
  * Twiddle tables are generated on the device once per (device, logN,
  * modulus) and kept resident in a process-wide registry shared by all
  * batches.  Jobs of one batch must not overlap in memory (operands may be
@@ -31,6 +34,7 @@ extern "C" {
 #define NTT_OP_FORWARD 0
 #define NTT_OP_INVERSE 1
 #define NTT_OP_MULTIPLY 2
+#define NTT_OP_MULTIPLY_SPECTRUM 3
 
 #define NTT_BATCH_MIN_LOGN 12
 #define NTT_BATCH_MAX_LOGN 17
@@ -41,8 +45,9 @@ typedef struct ntt_job {
     int limbs;                     /* >= 1 */
     const ModulusConfig* moduli;   /* host array [limbs]: the job's modulus chain */
     uint32_t* data;                /* device, limbs * 2^logN words, in place */
-    const uint32_t* operand;       /* NTT_OP_MULTIPLY: the other factor (device, same
-                                      shape); otherwise NULL */
+    const uint32_t* operand;       /* multiplies: the other factor (device, same shape;
+                                      its spectrum for NTT_OP_MULTIPLY_SPECTRUM);
+                                      otherwise NULL */
 } ntt_job_t;
 
 typedef struct ntt_batch_options {

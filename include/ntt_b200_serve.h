@@ -40,12 +40,13 @@ typedef struct ntt_server_options {
 } ntt_server_options_t;
 
 typedef struct ntt_request {
-    int op;                       /* NTT_OP_FORWARD / NTT_OP_INVERSE / NTT_OP_MULTIPLY */
+    int op;                       /* NTT_OP_FORWARD / _INVERSE / _MULTIPLY / _MULTIPLY_SPECTRUM */
     int logN;                     /* 12..17 */
     int limbs;
     const ModulusConfig* moduli;  /* [limbs]; copied at submit */
     const uint32_t* input;        /* host, limbs * 2^logN words */
-    const uint32_t* operand;      /* host: multiply's other factor (or use operand_handle) */
+    const uint32_t* operand;      /* host: multiply's other factor, a spectrum for
+                                     _MULTIPLY_SPECTRUM (or use operand_handle) */
     uint64_t operand_handle;      /* resident operand from ntt_server_put (0 = none) */
     uint32_t* output;             /* host, limbs * 2^logN words (may equal input) */
 } ntt_request_t;
@@ -56,7 +57,8 @@ typedef struct ntt_server_stats {
     double mean_round_requests;
     double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> results in the host buffer */
     double elapsed_s;             /* first submit -> last completion */
-    double limb_ntt_per_s;        /* completed limb transforms / elapsed (multiply = 3) */
+    double limb_ntt_per_s;        /* completed limb transforms / elapsed (multiply = 3,
+                                     spectrum multiply = 2) */
     size_t budget_bytes, arena_peak_bytes, resident_bytes, table_bytes;
 } ntt_server_stats_t;
 
@@ -75,6 +77,13 @@ NTT_API double ntt_server_latency_ms(ntt_server_t* s, uint64_t ticket);
 /* Copies `words` host words into the arena as a resident operand. */
 NTT_API ntt_status_t ntt_server_put(ntt_server_t* s, const uint32_t* host, size_t words,
                                     uint64_t* handle);
+/* Copies a polynomial of `limbs` x 2^logN host words into the arena and
+ * replaces it by its spectrum (forward transform), for
+ * NTT_OP_MULTIPLY_SPECTRUM requests: each multiply by it then costs two
+ * transforms instead of three.  Synchronous. */
+NTT_API ntt_status_t ntt_server_put_spectrum(ntt_server_t* s, int logN,
+                                             const ModulusConfig* moduli, int limbs,
+                                             const uint32_t* host, uint64_t* handle);
 NTT_API ntt_status_t ntt_server_drop(ntt_server_t* s, uint64_t handle);
 /* reset != 0 clears the latency record and counters after reading. */
 NTT_API ntt_status_t ntt_server_stats(ntt_server_t* s, int reset, ntt_server_stats_t* out);

@@ -425,6 +425,7 @@ def autotune_reload():
 OP_FORWARD = 0
 OP_INVERSE = 1
 OP_MULTIPLY = 2
+OP_MULTIPLY_SPECTRUM = 3
 BATCH_MIN_LOGN = 12
 BATCH_MAX_LOGN = 17
 
@@ -569,6 +570,8 @@ _sig("ntt_server_wait", _st, _vp, ctypes.c_uint64, ctypes.c_double)
 _sig("ntt_server_latency_ms", ctypes.c_double, _vp, ctypes.c_uint64)
 _sig("ntt_server_put", _st, _vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64))
 _sig("ntt_server_drop", _st, _vp, ctypes.c_uint64)
+_sig("ntt_server_put_spectrum", _st, _vp, ctypes.c_int, ctypes.POINTER(ModulusConfig), ctypes.c_int,
+     _vp, ctypes.POINTER(ctypes.c_uint64))
 _sig("ntt_server_stats", _st, _vp, ctypes.c_int, ctypes.POINTER(ServerStats))
 _sig("ntt_server_destroy", _st, _vp)
 
@@ -638,6 +641,14 @@ class Server:
         words = int(host.size) if hasattr(host, "size") and not callable(host.size) else host.numel()
         _check(_lib.ntt_server_put(self._h, _host_ptr(host), words, ctypes.byref(h)),
                "ntt_server_put")
+        return h.value
+
+    def put_spectrum(self, logN: int, moduli: Sequence, host) -> int:
+        """Resident operand stored as its spectrum (for OP_MULTIPLY_SPECTRUM)."""
+        m, n = _moduli_array(moduli)
+        h = ctypes.c_uint64()
+        _check(_lib.ntt_server_put_spectrum(self._h, logN, m, n, _host_ptr(host), ctypes.byref(h)),
+               "ntt_server_put_spectrum")
         return h.value
 
     def drop(self, handle: int):

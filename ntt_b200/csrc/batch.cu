@@ -18,10 +18,10 @@
 #include "runtime.h"
 
 namespace nttb {
-extern const void* const kBatchKernel_c16;
-extern const void* const kBatchKernel_c16m;
-extern const void* const kBatchKernel_c8;
-extern const void* const kBatchKernel_c8m;
+extern const void* const kBatchKernel_c16[2];
+extern const void* const kBatchKernel_c16m[2];
+extern const void* const kBatchKernel_c8[2];
+extern const void* const kBatchKernel_c8m[2];
 
 #define NTT_CUDA_TRY(expr, what)                         \
     do {                                                 \
@@ -148,9 +148,22 @@ void tables_trim() {
 // ---------------------------------------------------------------------------
 // Kernel variants.
 // ---------------------------------------------------------------------------
-const void* batch_kernel_fn(int cl, bool mul) {
-    if (cl == 16) return mul ? kBatchKernel_c16m : kBatchKernel_c16;
-    return mul ? kBatchKernel_c8m : kBatchKernel_c8;
+BatchVariant batch_variant(const BatchTile* tiles, size_t n, int cluster_ctas) {
+    BatchVariant v{cluster_ctas, false, false};
+    uint32_t max_logn = 0;
+    for (size_t i = 0; i < n; ++i) {
+        v.mul |= batch_op_is_multiply(tiles[i].op);
+        v.lazy2 |= tiles[i].q >= (1u << 30);
+        max_logn = tiles[i].logn > max_logn ? tiles[i].logn : max_logn;
+    }
+    if (!v.cluster_ctas) v.cluster_ctas = max_logn >= 17 ? 16 : 8;
+    return v;
+}
+
+const void* batch_kernel_fn(const BatchVariant& v) {
+    const int k = v.lazy2 ? 1 : 0;
+    if (v.cluster_ctas == 16) return v.mul ? kBatchKernel_c16m[k] : kBatchKernel_c16[k];
+    return v.mul ? kBatchKernel_c8m[k] : kBatchKernel_c8[k];
 }
 uint32_t batch_kernel_smem(bool mul) {
     return mul ? batch_smem_bytes<true>() : batch_smem_bytes<false>();
@@ -164,9 +177,10 @@ std::map<std::pair<int, const void*>, int> g_bk_occ;
 
 // Resident clusters of a batch-kernel variant on the current device (sets
 // the function attributes on first use).
-int batch_resident_clusters(int cl, bool mul) {
-    const void* fn = batch_kernel_fn(cl, mul);
-    const uint32_t smem = batch_kernel_smem(mul);
+int batch_resident_clusters(const BatchVariant& v) {
+    const int cl = v.cluster_ctas;
+    const void* fn = batch_kernel_fn(v);
+    const uint32_t smem = batch_kernel_smem(v.mul);
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     std::lock_guard<std::mutex> lk(g_bk_mu);
@@ -203,7 +217,9 @@ int batch_resident_clusters(int cl, bool mul) {
     return n;
 }
 
-ntt_status_t batch_launch(const BatchArgs& a, int cl, bool mul, int clusters, cudaStream_t s) {
+ntt_status_t batch_launch(const BatchArgs& a, const BatchVariant& v, int clusters, cudaStream_t s) {
+    const int cl = v.cluster_ctas;
+    const bool mul = v.mul;
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3(cl * clusters, 1, 1);
     lc.blockDim = dim3(kBatchThreads, 1, 1);
@@ -218,7 +234,7 @@ ntt_status_t batch_launch(const BatchArgs& a, int cl, bool mul, int clusters, cu
     lc.numAttrs = 1;
     BatchArgs copy = a;
     void* params[] = {&copy};
-    NTT_CUDA_TRY(cudaLaunchKernelExC(&lc, batch_kernel_fn(cl, mul), params), "batch kernel launch");
+    NTT_CUDA_TRY(cudaLaunchKernelExC(&lc, batch_kernel_fn(v), params), "batch kernel launch");
     return NTT_OK;
 }
 
@@ -264,6 +280,7 @@ struct ntt_batch {
     int device = 0;
     int jobs = 0, cl = 8, clusters = 0;
     bool mul = false;
+    BatchVariant variant{8, false, false};
     bool use_graph = true;
     std::vector<BatchTile> tiles;
     std::vector<uint32_t> slots, rounds;
@@ -290,7 +307,8 @@ static ntt_status_t batch_build(const ntt_job_t* jobs, int count, const ntt_batc
     size_t ntiles = 0;
     for (int j = 0; j < count; ++j) {
         const ntt_job_t& J = jobs[j];
-        if (J.op != NTT_OP_FORWARD && J.op != NTT_OP_INVERSE && J.op != NTT_OP_MULTIPLY)
+        if (J.op != NTT_OP_FORWARD && J.op != NTT_OP_INVERSE && J.op != NTT_OP_MULTIPLY &&
+            J.op != NTT_OP_MULTIPLY_SPECTRUM)
             return fail(NTT_ERR_INVALID_ARGUMENT, "job %d: unknown op %d", j, J.op);
         if (J.logN < NTT_BATCH_MIN_LOGN || J.logN > NTT_BATCH_MAX_LOGN)
             return fail(NTT_ERR_UNSUPPORTED, "job %d: logN %d outside [%d, %d]", j, J.logN,
@@ -299,7 +317,7 @@ static ntt_status_t batch_build(const ntt_job_t* jobs, int count, const ntt_batc
             return fail(NTT_ERR_INVALID_ARGUMENT, "job %d: needs limbs, moduli and data", j);
         if ((uintptr_t)J.data % 16)
             return fail(NTT_ERR_MISALIGNED, "job %d: data must be 16-byte aligned", j);
-        if (J.op == NTT_OP_MULTIPLY) {
+        if (batch_op_is_multiply((uint32_t)J.op)) {
             if (!J.operand) return fail(NTT_ERR_INVALID_ARGUMENT, "job %d: multiply needs an operand", j);
             if ((uintptr_t)J.operand % 16)
                 return fail(NTT_ERR_MISALIGNED, "job %d: operand must be 16-byte aligned", j);
@@ -329,7 +347,7 @@ static ntt_status_t batch_build(const ntt_job_t* jobs, int count, const ntt_batc
         for (int l = 0; l < J.limbs; ++l) {
             BatchTile t;
             t.data = J.data + (size_t)l * N;
-            t.operand = J.op == NTT_OP_MULTIPLY ? J.operand + (size_t)l * N : nullptr;
+            t.operand = batch_op_is_multiply((uint32_t)J.op) ? J.operand + (size_t)l * N : nullptr;
             t.tw_fwd = refs[l].fwd;
             t.tw_inv = refs[l].inv;
             t.q = refs[l].q;
@@ -361,7 +379,8 @@ static ntt_status_t batch_build(const ntt_job_t* jobs, int count, const ntt_batc
         NTT_CUDA_TRY(cudaMemcpy((void*)b->args.rounds, b->rounds.data(), groups * 4,
                                 cudaMemcpyHostToDevice), "batch upload");
     }
-    const int resident = batch_resident_clusters(cl, mul);
+    b->variant = batch_variant(b->tiles.data(), b->tiles.size(), cl);
+    const int resident = batch_resident_clusters(b->variant);
     if (resident <= 0) return fail(NTT_ERR_CUDA, "batch kernel: no resident clusters of %d CTAs", cl);
     int clusters = std::min<int>(resident, (int)groups);
     if (opt.max_clusters > 0) clusters = std::min(clusters, opt.max_clusters);
@@ -372,7 +391,7 @@ static ntt_status_t batch_build(const ntt_job_t* jobs, int count, const ntt_batc
 
 static ntt_status_t batch_enqueue(ntt_batch_t* b, cudaStream_t s) {
     NTT_CUDA_TRY(cudaMemsetAsync(b->args.counter, 0, 4, s), "batch counter reset");
-    return batch_launch(b->args, b->cl, b->mul, b->clusters, s);
+    return batch_launch(b->args, b->variant, b->clusters, s);
 }
 
 extern "C" {

@@ -18,8 +18,14 @@ constexpr int kBatchMaxLogN = 17;
 constexpr uint32_t kOpForward = 0;   // forward NTT in place
 constexpr uint32_t kOpInverse = 1;   // inverse NTT in place
 constexpr uint32_t kOpMultiply = 2;  // data = INTT(NTT(operand) . NTT(data))
+constexpr uint32_t kOpMultiplySpectrum = 3;  // data = INTT(operand . NTT(data)), operand a spectrum
+constexpr bool batch_op_is_multiply(uint32_t op) {
+    return op == kOpMultiply || op == kOpMultiplySpectrum;
+}
 // cluster barrier rounds a tile of each operation takes (one per transform)
-constexpr uint32_t batch_op_rounds(uint32_t op) { return op == kOpMultiply ? 3u : 1u; }
+constexpr uint32_t batch_op_rounds(uint32_t op) {
+    return op == kOpMultiply ? 3u : op == kOpMultiplySpectrum ? 2u : 1u;
+}
 // log2 CTAs per limb tile
 constexpr int batch_tile_clog(int logN) { return logN >= 14 ? logN - 13 : 0; }
 // slot word of a group: tile index | sub-rank << 24, or idle
@@ -30,11 +36,11 @@ constexpr int kSlotSubShift = 24;
 // One (polynomial, limb) tile.  48 bytes.
 struct BatchTile {
     uint32_t* data;           // limb start: input, output in place
-    const uint32_t* operand;  // kOpMultiply: the other factor's limb (read only)
+    const uint32_t* operand;  // multiplies: the other factor's limb (read only)
     const void* tw_fwd;       // [2^logN] forward Shoup twiddle pairs of this modulus
     const void* tw_inv;       // [2^logN] inverse pairs
     uint32_t q;               // modulus
-    uint32_t qinv;            // -q^{-1} mod 2^32 (kOpMultiply)
+    uint32_t qinv;            // -q^{-1} mod 2^32 (multiplies)
     uint32_t logn;
     uint32_t op;
 };

@@ -13,8 +13,15 @@
 // arrive (after its last local read of phase 1), one wait (before the DSMEM
 // scatter) and one release/acquire barrier (after the scatter).  A group's
 // CTAs all run the same number of such rounds (the group's `rounds`): a
-// multiply tile runs three bodies, a forward/inverse tile one, and any CTA
-// with fewer bodies (or no tile) runs empty rounds with the same barriers.
+// multiply tile runs three bodies (two when the operand is already a
+// spectrum), a forward/inverse tile one, and any CTA with fewer bodies (or
+// no tile) runs empty rounds with the same barriers.
+//
+// Multiply tiles pass their intermediate spectra through the tile's own
+// slab of the output limb in global memory (L2-resident between bodies):
+// every geometry gives CTA `rank` the same phase-2 slab and a CTA barrier
+// separates the bodies, so shared memory -- hence occupancy -- stays that
+// of a plain transform.
 // The index of the next group is fetched by CTA 0 during the current group
 // and stored into every CTA's slot word before the last round's release
 // barrier, so no extra barrier is spent on distributing work.
@@ -55,20 +62,23 @@ constexpr uint32_t kBatchWorkWords = (uint32_t)cmax<
          cmax<BatchGeo<16, false>::G::SMEM_WORDS, BatchGeo<15, true>::G::SMEM_WORDS>()>(),
     cmax<cmax<BatchGeo<14, true>::G::SMEM_WORDS, BatchGeo<13, true>::G::SMEM_WORDS>(),
          BatchGeo<12, true>::G::SMEM_WORDS>()>();
-constexpr uint32_t kBatchKeepWords = StageLayout::phys(8192u - 1u) + 1u;
-// dynamic shared memory: work buffer | keep buffer (multiply) | 2 slot words
+// dynamic shared memory: work buffer | 2 slot words (and padding)
 template <bool Mul>
 constexpr uint32_t batch_smem_words() {
-    return ((kBatchWorkWords + (Mul ? kBatchKeepWords : 0u)) + 3u & ~3u) + 4u;
+    return ((kBatchWorkWords + 3u) & ~3u) + 4u;
 }
 template <bool Mul>
 constexpr uint32_t batch_smem_bytes() {
     return 4u * batch_smem_words<Mul>();
 }
 
-// Where a body reads its input and writes its output.
-enum class BIn { Global, Keep };
-enum class BOut { Global, Keep, MulKeep };
+// Where a body reads its input and writes its output.  GlobalCG: a limb
+// slab this kernel wrote earlier (read through L2, not the read-only or L1
+// paths).  MulGlobal: the output word is the Montgomery product of the
+// transform's word and the word at the same offset of `gmul` (read first,
+// through L2), then stored to `gout`.
+enum class BIn { Global, GlobalCG };
+enum class BOut { Global, MulGlobal };
 
 // Hand-off of the next group index: CTA 0's thread 0 stores `value` into the
 // slot word at `slot_sa` of every CTA of the cluster.
@@ -96,36 +106,31 @@ __device__ __forceinline__ void bcast_release(const Bcast& bc) {
 }
 
 // Memory interface of one tile body (see DevCtx for the pass code's use).
-// The keep buffer holds this CTA's M words of a phase-2 slab at
-// StageLayout::phys(lambda) (one pad per 128 bytes).
 template <class G, int CL, BIn IM, BOut OM>
 struct BatchCtx {
     static constexpr bool kStaged = false;
     static constexpr int C = G::C;
     const uint32_t* __restrict__ gin;
-    uint32_t* __restrict__ gout;
+    uint32_t* gout;
+    const uint32_t* gmul;
     const TwPair* __restrict__ twp;
     uint32_t* smem;
-    uint32_t* keep;
     const uint32_t* stage;  // unused (direct input)
     uint32_t smem_sa;
     uint32_t q, q2, qinv, rank, base;
     Bcast bc;
 
     // ---- input ----
-    __device__ __forceinline__ const uint32_t* g_base(uint32_t o) const {
-        if constexpr (IM == BIn::Global) return gin + o;
-        else return keep + StageLayout::phys(o - rank * G::M);
-    }
+    __device__ __forceinline__ const uint32_t* g_base(uint32_t o) const { return gin + o; }
     __device__ __forceinline__ uint32_t g_ld(const uint32_t* b, uint32_t c) const {
         if constexpr (IM == BIn::Global) return __ldca(b + c);
-        else return b[StageLayout::phys(c)];
+        else return __ldcg(b + c);
     }
     __device__ __forceinline__ void g_ld4(const uint32_t* b, uint32_t c, uint32_t& x, uint32_t& y,
                                           uint32_t& z, uint32_t& w) const {
         uint4 t;
         if constexpr (IM == BIn::Global) t = __ldca(reinterpret_cast<const uint4*>(b + c));
-        else t = *reinterpret_cast<const uint4*>(b + StageLayout::phys(c));
+        else t = __ldcg(reinterpret_cast<const uint4*>(b + c));
         x = t.x;
         y = t.y;
         z = t.z;
@@ -136,36 +141,24 @@ struct BatchCtx {
     __device__ __forceinline__ void st_ld4(const uint32_t*, uint32_t, uint32_t&, uint32_t&,
                                            uint32_t&, uint32_t&) const {}
     // ---- output ----
-    __device__ __forceinline__ uint32_t* o_base(uint32_t o) const {
-        if constexpr (OM == BOut::Global) return gout + o;
-        else return keep + StageLayout::phys(o - rank * G::M);
-    }
+    __device__ __forceinline__ uint32_t* o_base(uint32_t o) const { return gout + o; }
     __device__ __forceinline__ uint32_t mix(uint32_t v, uint32_t k) const {
         return mont_mul(v, k, q, qinv);
     }
     __device__ __forceinline__ void o_st(uint32_t* b, uint32_t c, uint32_t v) const {
-        if constexpr (OM == BOut::Global) {
-            b[c] = v;
-        } else {
-            uint32_t* p = b + StageLayout::phys(c);
-            *p = (OM == BOut::Keep) ? v : mix(v, *p);
-        }
+        if constexpr (OM == BOut::MulGlobal) v = mix(v, __ldcg(gmul + (b - gout) + c));
+        b[c] = v;
     }
     __device__ __forceinline__ void o_st4(uint32_t* b, uint32_t c, uint32_t x, uint32_t y,
                                           uint32_t z, uint32_t w) const {
-        if constexpr (OM == BOut::Global) {
-            *reinterpret_cast<uint4*>(b + c) = make_uint4(x, y, z, w);
-        } else {
-            uint4* p = reinterpret_cast<uint4*>(b + StageLayout::phys(c));
-            if constexpr (OM == BOut::MulKeep) {
-                const uint4 k = *p;
-                x = mix(x, k.x);
-                y = mix(y, k.y);
-                z = mix(z, k.z);
-                w = mix(w, k.w);
-            }
-            *p = make_uint4(x, y, z, w);
+        if constexpr (OM == BOut::MulGlobal) {
+            const uint4 k = __ldcg(reinterpret_cast<const uint4*>(gmul + (b - gout) + c));
+            x = mix(x, k.x);
+            y = mix(y, k.y);
+            z = mix(z, k.z);
+            w = mix(w, k.w);
         }
+        *reinterpret_cast<uint4*>(b + c) = make_uint4(x, y, z, w);
     }
     // ---- work buffer and scatter ----
     __device__ __forceinline__ uint32_t* s_base(uint32_t w) const { return smem + w; }
@@ -228,7 +221,6 @@ struct NoPrefetch {
 // Per-CTA state shared by the bodies of a tile.
 struct BatchCta {
     uint32_t* smem;
-    uint32_t* keep;
     uint32_t smem_sa;
     uint32_t rank;  // in the cluster
 };
@@ -242,18 +234,36 @@ __device__ __forceinline__ const void* reload_ptr(const void* const* addr) {
     asm volatile("ld.volatile.global.u64 %0, [%1];" : "=l"(v) : "l"(addr));
     return reinterpret_cast<const void*>(v);
 }
+// A tile re-read field by field before each body of a multiply, so that no
+// field stays live in registers across a body.
+__device__ __forceinline__ BatchTile reload_tile(const BatchTile* tp) {
+    BatchTile t;
+    t.data = (uint32_t*)reload_ptr((const void* const*)&tp->data);
+    t.operand = (const uint32_t*)reload_ptr((const void* const*)&tp->operand);
+    t.tw_fwd = reload_ptr(&tp->tw_fwd);
+    t.tw_inv = reload_ptr(&tp->tw_inv);
+    uint32_t q, qinv;
+    asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(q) : "l"(&tp->q));
+    asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(qinv) : "l"(&tp->qinv));
+    t.q = q;
+    t.qinv = qinv;
+    t.logn = 0;
+    t.op = 0;
+    return t;
+}
 
 template <class G, int CL, BIn IM, BOut OM>
 __device__ __forceinline__ BatchCtx<G, CL, IM, OM> make_ctx(const BatchCta& cta,
                                                             const BatchTile& t, uint32_t sub,
                                                             const uint32_t* in, uint32_t* out,
-                                                            const void* tw, const Bcast& bc) {
+                                                            const uint32_t* mul, const void* tw,
+                                                            const Bcast& bc) {
     BatchCtx<G, CL, IM, OM> c;
     c.gin = in;
     c.gout = out;
+    c.gmul = mul;
     c.twp = reinterpret_cast<const TwPair*>(tw);
     c.smem = cta.smem;
-    c.keep = cta.keep;
     c.stage = nullptr;
     c.smem_sa = cta.smem_sa;
     c.q = t.q;
@@ -279,77 +289,103 @@ __device__ __forceinline__ uint32_t run_tile_arith(const BatchCta& cta, const Ba
     };
     if (t.op == kOpForward) {
         using G = typename BatchGeo<LOGN, true>::G;
-        auto c = make_ctx<G, CL, BIn::Global, BOut::Global>(cta, t, sub, t.data, t.data, t.tw_fwd,
-                                                            round_bc(0));
+        auto c = make_ctx<G, CL, BIn::Global, BOut::Global>(cta, t, sub, t.data, t.data, nullptr,
+                                                            t.tw_fwd, round_bc(0));
         fused_forward_body<G, Arith>(c, NoPrefetch{});
         __syncthreads();
         return 1;
     }
     if (t.op == kOpInverse) {
         using G = typename BatchGeo<LOGN, false>::G;
-        auto c = make_ctx<G, CL, BIn::Global, BOut::Global>(cta, t, sub, t.data, t.data, t.tw_inv,
-                                                            round_bc(0));
+        auto c = make_ctx<G, CL, BIn::Global, BOut::Global>(cta, t, sub, t.data, t.data, nullptr,
+                                                            t.tw_inv, round_bc(0));
         fused_inverse_body<G, Arith>(c, NoPrefetch{});
         __syncthreads();
         return 1;
     }
     if constexpr (Mul) {
+        // forward bodies use the forward geometry, the inverse body the
+        // inverse one: both give CTA `rank` the same phase-2 slab
+        // [rank * M, (rank + 1) * M) (same cluster size), and the CTA barrier
+        // between bodies makes the slab written by one body visible to every
+        // thread of the next
+        using G = typename BatchGeo<LOGN, true>::G;
+        using GI = typename BatchGeo<LOGN, false>::G;
+        static_assert(G::CLOG == GI::CLOG && G::M == GI::M, "multiply bodies share CTA slabs");
         if (t.op == kOpMultiply) {
-            // one geometry for all three bodies: the forward's last pass and
-            // the inverse's first pass then own the same words per thread,
-            // so the keep buffer is only ever touched by its owner thread
-            using G = typename BatchGeo<LOGN, true>::G;
-            auto ca = make_ctx<G, CL, BIn::Global, BOut::Keep>(cta, t, sub, t.operand, nullptr,
-                                                               t.tw_fwd, round_bc(0));
-            fused_forward_body<G, Arith>(ca, NoPrefetch{});
-            __syncthreads();
-            auto cb = make_ctx<G, CL, BIn::Global, BOut::MulKeep>(
-                cta, t, sub, t.data, nullptr, reload_ptr(&tp->tw_fwd), round_bc(1));
-            fused_forward_body<G, Arith>(cb, NoPrefetch{});
-            __syncthreads();
-            auto cc = make_ctx<G, CL, BIn::Keep, BOut::Global>(cta, t, sub, nullptr, t.data,
-                                                               t.tw_inv, round_bc(2));
-            fused_inverse_body<G, Arith>(cc, NoPrefetch{});
-            __syncthreads();
+            {   // b -> spectrum of b, in place
+                const BatchTile u = reload_tile(tp);
+                auto cb = make_ctx<G, CL, BIn::Global, BOut::Global>(cta, u, sub, u.data, u.data,
+                                                                     nullptr, u.tw_fwd,
+                                                                     round_bc(0));
+                fused_forward_body<G, Arith>(cb, NoPrefetch{});
+                __syncthreads();
+            }
+            {   // spectrum of a times spectrum of b, into b's slab
+                const BatchTile u = reload_tile(tp);
+                auto ca = make_ctx<G, CL, BIn::Global, BOut::MulGlobal>(
+                    cta, u, sub, u.operand, u.data, u.data, u.tw_fwd, round_bc(1));
+                fused_forward_body<G, Arith>(ca, NoPrefetch{});
+                __syncthreads();
+            }
+            {
+                const BatchTile u = reload_tile(tp);
+                auto cc = make_ctx<GI, CL, BIn::GlobalCG, BOut::Global>(
+                    cta, u, sub, u.data, u.data, nullptr, u.tw_inv, round_bc(2));
+                fused_inverse_body<GI, Arith>(cc, NoPrefetch{});
+                __syncthreads();
+            }
             return 3;
+        }
+        if (t.op == kOpMultiplySpectrum) {
+            {
+                const BatchTile u = reload_tile(tp);
+                auto cb = make_ctx<G, CL, BIn::Global, BOut::MulGlobal>(
+                    cta, u, sub, u.data, u.data, u.operand, u.tw_fwd, round_bc(0));
+                fused_forward_body<G, Arith>(cb, NoPrefetch{});
+                __syncthreads();
+            }
+            {
+                const BatchTile u = reload_tile(tp);
+                auto cc = make_ctx<GI, CL, BIn::GlobalCG, BOut::Global>(
+                    cta, u, sub, u.data, u.data, nullptr, u.tw_inv, round_bc(1));
+                fused_inverse_body<GI, Arith>(cc, NoPrefetch{});
+                __syncthreads();
+            }
+            return 2;
         }
     }
     return 0;
 }
 
-template <int LOGN, int CL, bool Mul>
-__device__ __forceinline__ uint32_t run_tile_n(const BatchCta& cta, const BatchTile& t,
-                                               const BatchTile* tp, uint32_t sub, uint32_t last,
-                                               Bcast bc) {
-    if (t.q < (1u << 30)) return run_tile_arith<LOGN, CL, Mul, Lazy4>(cta, t, tp, sub, last, bc);
-    return run_tile_arith<LOGN, CL, Mul, Lazy2>(cta, t, tp, sub, last, bc);
-}
-
-template <int CL, bool Mul>
+template <int CL, bool Mul, class Arith>
 __device__ __forceinline__ uint32_t run_tile(const BatchCta& cta, const BatchTile* tp,
                                              uint32_t sub, uint32_t last, Bcast bc) {
     const BatchTile t = *tp;
     switch (t.logn) {
-        case 12: return run_tile_n<12, CL, Mul>(cta, t, tp, sub, last, bc);
-        case 13: return run_tile_n<13, CL, Mul>(cta, t, tp, sub, last, bc);
-        case 14: return run_tile_n<14, CL, Mul>(cta, t, tp, sub, last, bc);
-        case 15: return run_tile_n<15, CL, Mul>(cta, t, tp, sub, last, bc);
-        case 16: return run_tile_n<16, CL, Mul>(cta, t, tp, sub, last, bc);
+        case 12: return run_tile_arith<12, CL, Mul, Arith>(cta, t, tp, sub, last, bc);
+        case 13: return run_tile_arith<13, CL, Mul, Arith>(cta, t, tp, sub, last, bc);
+        case 14: return run_tile_arith<14, CL, Mul, Arith>(cta, t, tp, sub, last, bc);
+        case 15: return run_tile_arith<15, CL, Mul, Arith>(cta, t, tp, sub, last, bc);
+        case 16: return run_tile_arith<16, CL, Mul, Arith>(cta, t, tp, sub, last, bc);
         case 17:
-            if constexpr (CL >= 16) return run_tile_n<17, CL, Mul>(cta, t, tp, sub, last, bc);
+            if constexpr (CL >= 16) return run_tile_arith<17, CL, Mul, Arith>(cta, t, tp, sub, last, bc);
             else return 0;
         default: return 0;
     }
 }
 
-// grid.x = CL * resident clusters; cluster dims (CL, 1, 1).
-template <int CL, bool Mul>
-__global__ void __launch_bounds__(kBatchThreads, Mul ? 3 : 4) batch_kernel(BatchArgs a) {
+// grid.x = CL * resident clusters; cluster dims (CL, 1, 1).  Arith: the
+// range discipline of every tile of the launch (Lazy4 when all moduli are
+// below 2^30, else Lazy2), fixed per kernel so that one path's registers fit
+// the launch bounds (4 CTAs/SM: the persistent loop's own state does not fit
+// the 48 registers of 5).
+template <int CL, bool Mul, class Arith>
+__global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(BatchArgs a) {
     extern __shared__ __align__(16) uint32_t smem[];
     constexpr uint32_t kSlotOff = batch_smem_words<Mul>() - 4u;
     BatchCta cta;
     cta.smem = smem;
-    cta.keep = smem + kBatchWorkWords;
     cta.smem_sa = (uint32_t)__cvta_generic_to_shared(smem);
     cta.rank = cluster_rank();
     const uint32_t slot_sa = cta.smem_sa + 4u * kSlotOff;
@@ -375,7 +411,7 @@ __global__ void __launch_bounds__(kBatchThreads, Mul ? 3 : 4) batch_kernel(Batch
         const Bcast bc{nxt, slot_sa + 4u * ((it + 1u) & 1u), leader};
         uint32_t done = 0;
         if (sl != kIdleSlot) {
-            done = run_tile<CL, Mul>(cta, a.tiles + (sl & kSlotTileMask), sl >> kSlotSubShift,
+            done = run_tile<CL, Mul, Arith>(cta, a.tiles + (sl & kSlotTileMask), sl >> kSlotSubShift,
                                      rounds - 1u, bc);
         }
         for (uint32_t r = done; r < rounds; ++r) {

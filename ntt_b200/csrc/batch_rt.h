@@ -40,12 +40,18 @@ bool find_resident_table(int device, int logN, ModulusConfig m, const TwPair** f
                          const TwPair** inv, uint32_t* nqinv);
 void tables_trim();
 
-const void* batch_kernel_fn(int cluster_ctas, bool mul);
+// Which instantiation of the batch kernel a launch needs.
+struct BatchVariant {
+    int cluster_ctas;  // 8 or 16 (16 when a tile has logN 17)
+    bool mul;          // multiply tiles present
+    bool lazy2;        // a modulus >= 2^30: [0, 2q) range discipline for every tile
+};
+BatchVariant batch_variant(const BatchTile* tiles, size_t n, int cluster_ctas);
+const void* batch_kernel_fn(const BatchVariant& v);
 uint32_t batch_kernel_smem(bool mul);
-int batch_resident_clusters(int cluster_ctas, bool mul);
+int batch_resident_clusters(const BatchVariant& v);
 // One persistent launch (the counter must be zero, e.g. a memset ahead of it).
-ntt_status_t batch_launch(const BatchArgs& a, int cluster_ctas, bool mul, int clusters,
-                          cudaStream_t s);
+ntt_status_t batch_launch(const BatchArgs& a, const BatchVariant& v, int clusters, cudaStream_t s);
 // Groups of cluster_ctas slots for the tiles (see batch.cu).
 void pack_tiles(const std::vector<BatchTile>& tiles, int cluster_ctas,
                 std::vector<uint32_t>& slots, std::vector<uint32_t>& rounds);

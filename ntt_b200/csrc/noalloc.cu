@@ -81,7 +81,7 @@ ntt_status_t scratch_ptr(int dev, unsigned char** out) {
 // filling as the allocating path, into the static arrays.  Returns groups.
 uint32_t pack_static(uint32_t ntiles, int cl) {
     uint32_t n = 0;
-    for (int r = 3; r >= 1; r -= 2)
+    for (int r = 3; r >= 1; --r)
         for (int lg = kBatchMaxLogN; lg >= kBatchMinLogN; --lg)
             for (uint32_t t = 0; t < ntiles; ++t)
                 if ((int)batch_op_rounds(g_host.tiles[t].op) == r && (int)g_host.tiles[t].logn == lg)
@@ -113,10 +113,10 @@ extern "C" ntt_status_t ntt_batch_run_noalloc(const ntt_job_t* jobs, int count,
     if (count < 0 || (count > 0 && !jobs)) return fail(NTT_ERR_INVALID_ARGUMENT, "bad job array");
     uint64_t ntiles = 0;
     int max_logn = 0;
-    bool mul = false;
     for (int j = 0; j < count; ++j) {
         const ntt_job_t& J = jobs[j];
-        if (J.op != NTT_OP_FORWARD && J.op != NTT_OP_INVERSE && J.op != NTT_OP_MULTIPLY)
+        if (J.op != NTT_OP_FORWARD && J.op != NTT_OP_INVERSE && J.op != NTT_OP_MULTIPLY &&
+            J.op != NTT_OP_MULTIPLY_SPECTRUM)
             return fail(NTT_ERR_INVALID_ARGUMENT, "job %d: unknown op %d", j, J.op);
         if (J.logN < NTT_BATCH_MIN_LOGN || J.logN > NTT_BATCH_MAX_LOGN)
             return fail(NTT_ERR_UNSUPPORTED, "job %d: logN %d outside [%d, %d]", j, J.logN,
@@ -125,11 +125,10 @@ extern "C" ntt_status_t ntt_batch_run_noalloc(const ntt_job_t* jobs, int count,
             return fail(NTT_ERR_INVALID_ARGUMENT, "job %d: needs limbs, moduli and data", j);
         if ((uintptr_t)J.data % 16)
             return fail(NTT_ERR_MISALIGNED, "job %d: data must be 16-byte aligned", j);
-        if (J.op == NTT_OP_MULTIPLY) {
+        if (batch_op_is_multiply((uint32_t)J.op)) {
             if (!J.operand) return fail(NTT_ERR_INVALID_ARGUMENT, "job %d: multiply needs an operand", j);
             if ((uintptr_t)J.operand % 16)
                 return fail(NTT_ERR_MISALIGNED, "job %d: operand must be 16-byte aligned", j);
-            mul = true;
         }
         if (J.logN > max_logn) max_logn = J.logN;
         ntiles += (uint64_t)J.limbs;
@@ -160,7 +159,7 @@ extern "C" ntt_status_t ntt_batch_run_noalloc(const ntt_job_t* jobs, int count,
                             j, l, J.moduli[l].qi, J.logN);
             BatchTile& b = g_host.tiles[t];
             b.data = J.data + (size_t)l * N;
-            b.operand = J.op == NTT_OP_MULTIPLY ? J.operand + (size_t)l * N : nullptr;
+            b.operand = batch_op_is_multiply((uint32_t)J.op) ? J.operand + (size_t)l * N : nullptr;
             b.tw_fwd = fwd;
             b.tw_inv = inv;
             b.q = J.moduli[l].qi;
@@ -186,7 +185,8 @@ extern "C" ntt_status_t ntt_batch_run_noalloc(const ntt_job_t* jobs, int count,
                             cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(a.counter, 0, 4, s);
     if (e != cudaSuccess) return cuda_fail(e, "scratch upload");
-    const int resident = batch_resident_clusters(cl, mul);
+    const BatchVariant v = batch_variant(g_host.tiles, (size_t)ntiles, cl);
+    const int resident = batch_resident_clusters(v);
     if (resident <= 0) return fail(NTT_ERR_CUDA, "batch kernel: no resident clusters of %d CTAs", cl);
-    return batch_launch(a, cl, mul, resident < (int)groups ? resident : (int)groups, s);
+    return batch_launch(a, v, resident < (int)groups ? resident : (int)groups, s);
 }

@@ -86,7 +86,9 @@ struct Req {
     std::vector<TableRef> tables;
     Clock::time_point t_submit, t_done;
     ntt_status_t status = NTT_ERR_NOT_READY;
-    size_t arena_need() const { return bytes + (op == NTT_OP_MULTIPLY && !operand_handle ? bytes : 0); }
+    size_t arena_need() const {
+        return bytes + (batch_op_is_multiply((uint32_t)op) && !operand_handle ? bytes : 0);
+    }
 };
 using ReqP = std::shared_ptr<Req>;
 
@@ -150,7 +152,7 @@ void finish_round(ntt_server* S, Slot& sl, ntt_status_t st) {
         if (st == NTT_OK) {
             ++S->completed;
             S->lat_ms.push_back(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
-            S->limb_ntts += (double)r->limbs * (r->op == NTT_OP_MULTIPLY ? 3.0 : 1.0);
+            S->limb_ntts += (double)r->limbs * batch_op_rounds((uint32_t)r->op);
         } else {
             ++S->failed;
         }
@@ -169,14 +171,12 @@ ntt_status_t issue_round(ntt_server* S, Slot& sl) {
     cudaStream_t s = sl.stream;
     std::vector<BatchTile> tiles;
     int max_logn = 0;
-    bool mul = false;
     for (auto& r : sl.reqs) {
         char* data = S->arena_base + r->off_data;
         if (cudaMemcpyAsync(data, r->input, r->bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
             return cuda_fail(cudaGetLastError(), "round input copy");
         const uint32_t* opnd = nullptr;
-        if (r->op == NTT_OP_MULTIPLY) {
-            mul = true;
+        if (batch_op_is_multiply((uint32_t)r->op)) {
             if (r->operand_handle) {
                 opnd = (const uint32_t*)(S->arena_base + r->res_off);
             } else {
@@ -223,9 +223,10 @@ ntt_status_t issue_round(ntt_server* S, Slot& sl) {
     a.rounds = (const uint32_t*)(d + t_bytes + s_bytes);
     a.counter = (uint32_t*)(d + t_bytes + s_bytes + r_bytes);
     a.groups = (uint32_t)rounds.size();
-    const int resident = batch_resident_clusters(cl, mul);
+    const BatchVariant v = batch_variant(tiles.data(), tiles.size(), cl);
+    const int resident = batch_resident_clusters(v);
     if (resident <= 0) return fail(NTT_ERR_CUDA, "batch kernel: no resident clusters");
-    if (ntt_status_t st = batch_launch(a, cl, mul, std::min<int>(resident, (int)rounds.size()), s))
+    if (ntt_status_t st = batch_launch(a, v, std::min<int>(resident, (int)rounds.size()), s))
         return st;
     for (auto& r : sl.reqs)
         if (cudaMemcpyAsync(r->output, S->arena_base + r->off_data, r->bytes,
@@ -275,7 +276,7 @@ void scheduler_main(ntt_server* S) {
             const size_t od = S->arena.alloc(r->bytes);
             if (od == kNone) break;
             size_t oo = kNone;
-            if (r->op == NTT_OP_MULTIPLY) {
+            if (batch_op_is_multiply((uint32_t)r->op)) {
                 if (r->operand_handle) {
                     auto it = S->resident.find(r->operand_handle);
                     if (it == S->resident.end() || it->second.second < r->bytes) {
@@ -394,7 +395,8 @@ ntt_status_t ntt_server_create(const ntt_server_options_t* opts, ntt_server_t** 
 
 ntt_status_t ntt_server_submit(ntt_server_t* S, const ntt_request_t* q, uint64_t* ticket) {
     if (!S || !q || !ticket) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (q->op != NTT_OP_FORWARD && q->op != NTT_OP_INVERSE && q->op != NTT_OP_MULTIPLY)
+    if (q->op != NTT_OP_FORWARD && q->op != NTT_OP_INVERSE && q->op != NTT_OP_MULTIPLY &&
+        q->op != NTT_OP_MULTIPLY_SPECTRUM)
         return fail(NTT_ERR_INVALID_ARGUMENT, "unknown op %d", q->op);
     if (q->logN < NTT_BATCH_MIN_LOGN || q->logN > NTT_BATCH_MAX_LOGN)
         return fail(NTT_ERR_UNSUPPORTED, "logN %d outside [%d, %d]", q->logN, NTT_BATCH_MIN_LOGN,
@@ -405,7 +407,7 @@ ntt_status_t ntt_server_submit(ntt_server_t* S, const ntt_request_t* q, uint64_t
         return fail(NTT_ERR_INVALID_ARGUMENT, "request needs limbs, moduli, input and output");
     if (q->limbs > S->opt.max_round_tiles)
         return fail(NTT_ERR_UNSUPPORTED, "more limbs than a round holds (%d)", S->opt.max_round_tiles);
-    if (q->op == NTT_OP_MULTIPLY && !q->operand && !q->operand_handle)
+    if (batch_op_is_multiply((uint32_t)q->op) && !q->operand && !q->operand_handle)
         return fail(NTT_ERR_INVALID_ARGUMENT, "multiply needs an operand");
     auto r = std::make_shared<Req>();
     r->op = q->op;
@@ -413,7 +415,7 @@ ntt_status_t ntt_server_submit(ntt_server_t* S, const ntt_request_t* q, uint64_t
     r->limbs = q->limbs;
     r->input = q->input;
     r->operand = q->operand;
-    r->operand_handle = q->op == NTT_OP_MULTIPLY ? q->operand_handle : 0;
+    r->operand_handle = batch_op_is_multiply((uint32_t)q->op) ? q->operand_handle : 0;
     r->output = q->output;
     r->bytes = ((size_t)q->limbs << q->logN) * 4;
     if (r->arena_need() > S->arena_size)
@@ -501,6 +503,44 @@ ntt_status_t ntt_server_put(ntt_server_t* S, const uint32_t* host, size_t words,
     *handle = S->next_handle++;
     S->resident[*handle] = {off, words * 4};
     S->resident_bytes += (words * 4 + kAlign - 1) & ~(kAlign - 1);
+    return NTT_OK;
+}
+
+ntt_status_t ntt_server_put_spectrum(ntt_server_t* S, int logN, const ModulusConfig* moduli,
+                                     int limbs, const uint32_t* host, uint64_t* handle) {
+    if (!S || !moduli || !host || !handle || limbs < 1)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "bad arguments");
+    if (logN < NTT_BATCH_MIN_LOGN || logN > NTT_BATCH_MAX_LOGN)
+        return fail(NTT_ERR_UNSUPPORTED, "logN %d outside [%d, %d]", logN, NTT_BATCH_MIN_LOGN,
+                    NTT_BATCH_MAX_LOGN);
+    uint64_t h = 0;
+    if (ntt_status_t st = ntt_server_put(S, host, (size_t)limbs << logN, &h)) return st;
+    size_t off;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        off = S->resident[h].first;
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != S->device) cudaSetDevice(S->device);
+    ntt_job_t job{NTT_OP_FORWARD, logN, limbs, moduli, (uint32_t*)(S->arena_base + off), nullptr};
+    ntt_batch_options_t o{0, 0, 0};
+    ntt_batch_t* b = nullptr;
+    ntt_status_t st = ntt_batch_create(&job, 1, &o, &b);
+    cudaStream_t s = nullptr;
+    if (st == NTT_OK && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+        st = cuda_fail(cudaGetLastError(), "spectrum stream");
+    if (st == NTT_OK) st = ntt_batch_run(b, s);
+    if (st == NTT_OK && cudaStreamSynchronize(s) != cudaSuccess)
+        st = cuda_fail(cudaGetLastError(), "spectrum transform");
+    if (s) cudaStreamDestroy(s);
+    if (b) ntt_batch_destroy(b);
+    if (cur != S->device) cudaSetDevice(cur);
+    if (st != NTT_OK) {
+        ntt_server_drop(S, h);
+        return st;
+    }
+    *handle = h;
     return NTT_OK;
 }
 

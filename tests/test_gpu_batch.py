@@ -264,3 +264,28 @@ def test_pointwise_mul_matches_numpy(torch_cuda, nb, mixes):
     for i in range(2):
         assert np.array_equal(host(z)[i], mont_pointwise(host(x)[i], host(y)[i], mods))
     p.close()
+
+
+def test_multiply_spectrum_operand(torch_cuda, nb, mixes):
+    """OP_MULTIPLY_SPECTRUM with the operand given as its forward transform
+    equals OP_MULTIPLY with the operand itself (and the plain path)."""
+    torch = torch_cuda
+    jobs = mixes.ragged_mix(seed=21, count=20, logn=range(12, 18), limbs=(1, 4), bits=(30, 31),
+                            ops=((nb.OP_MULTIPLY, 1),))
+    data, ops = make_inputs(torch, mixes, jobs, 11)
+    expect = [plain_expected(torch, nb, j, x, a) for j, x, a in zip(jobs, data, ops)]
+    spectra = []
+    for j, a in zip(jobs, ops):
+        p = nb.Plan(j.logN, j.moduli)
+        s = a.clone()
+        p.forward(s)
+        spectra.append(s)
+        p.close()
+    torch.cuda.synchronize()
+    mixed = [(nb.OP_MULTIPLY_SPECTRUM if i % 2 == 0 else nb.OP_MULTIPLY, j.logN, j.moduli, x,
+              spectra[i] if i % 2 == 0 else ops[i]) for i, (j, x) in enumerate(zip(jobs, data))]
+    with nb.Batch(mixed) as b:
+        b.run()
+        torch.cuda.synchronize()
+    for i, x in enumerate(data):
+        assert np.array_equal(host(x), expect[i]), f"job {i}"

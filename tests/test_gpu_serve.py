@@ -175,6 +175,25 @@ def test_resident_operand(torch_cuda, nb, mixes):
         assert np.array_equal(o, plain(torch, nb, j, x, a))
 
 
+def test_resident_spectrum_operand(torch_cuda, nb, mixes):
+    torch = torch_cuda
+    j = mixes.ragged_mix(seed=37, count=1, logn=(15,), limbs=(3, 3),
+                         ops=((nb.OP_MULTIPLY, 1),))[0]
+    rng = np.random.default_rng(6)
+    a = rand_poly(rng, j)
+    with nb.Server(hbm_budget_bytes=256 << 20) as srv:
+        h = srv.put_spectrum(j.logN, j.moduli, a)
+        xs = [rand_poly(rng, j) for _ in range(5)]
+        outs = [np.empty_like(x) for x in xs]
+        ts = [srv.submit(nb.OP_MULTIPLY_SPECTRUM, j.logN, j.moduli, x, o, operand_handle=h)
+              for x, o in zip(xs, outs)]
+        for t in ts:
+            srv.wait(t, 60.0)
+        srv.drop(h)
+    for x, o in zip(xs, outs):
+        assert np.array_equal(o, plain(torch, nb, j, x, a))
+
+
 def test_in_place_output_and_errors(torch_cuda, nb, mixes):
     j = mixes.ragged_mix(seed=36, count=1, logn=(12,), limbs=(3, 3))[0]
     rng = np.random.default_rng(5)
