@@ -177,6 +177,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value_ms: float, device: str = "cuda") -> float:
+    """The job's time: the slowest rank's (a no-op with one process)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value_ms)
+    t = torch.tensor([float(value_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -250,10 +261,7 @@ def run_ours(args):
     elapsed_ms = t_start.elapsed_time(t_end)
     fwd_ms = np.array([ev[4 * k].elapsed_time(ev[4 * k + 1]) for k in range(K)])
     inv_ms = np.array([ev[4 * k + 2].elapsed_time(ev[4 * k + 3]) for k in range(K)])
-    t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_max = float(t.item())
+    elapsed_max = max_over_ranks(elapsed_ms)
 
     # e2e through the public API with host buffers (pinned), copies timed
     E = max(1, args.e2e_steps)
@@ -269,15 +277,13 @@ def run_ours(args):
             host_out.copy_(d, non_blocking=True)
         e1.record(stream)
     stream.synchronize()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     if not torch.equal(host_out, host_in):
         raise RuntimeError("e2e roundtrip is not the identity")
 
     transforms = 2 * P * LIMBS * K * world
     value = transforms / (elapsed_max / 1000.0)
-    e2e_value = 2 * P * LIMBS * E * world / (float(e2e_ms.item()) / 1000.0)
+    e2e_value = 2 * P * LIMBS * E * world / (e2e_ms / 1000.0)
 
     # roofline of the dominant kernel: algorithmic bytes = read + write of
     # every word once per launch (8 bytes per coefficient)
