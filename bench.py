@@ -452,7 +452,9 @@ def bench_multiply(args, torch, nb, stream):
     multiply tiles (NTT(a), NTT(b), pointwise Montgomery product, INTT per
     limb, a read once, b read and overwritten once).  Unfused: the plain
     calls forward_many(a), forward_many(b), pointwise_mul, inverse_many(b)
-    (4 launches; a is overwritten by its spectrum, which favours it)."""
+    (4 launches; a is overwritten by its spectrum, which favours it).  Plan
+    form: multiply_many (3 launches of the plain transform kernels: NTT(b),
+    NTT(a) with the pointwise product folded into its store, INTT(b))."""
     from ntt_b200 import mixes
     logN, limbs, pairs = 16, 24, 128
     mods = list(mixes.prime_pool(logN, 30, limbs))
@@ -476,6 +478,12 @@ def bench_multiply(args, torch, nb, stream):
     stream.synchronize()
     if not torch.equal(b, tb):
         raise RuntimeError("fused and unfused multiply differ")
+    pb = b0.clone()
+    with torch.cuda.stream(stream):
+        p.multiply_many(a, pb, pairs, 0, sh)
+    stream.synchronize()
+    if not torch.equal(pb, tb):
+        raise RuntimeError("plan-level and unfused multiply differ")
     del b0
 
     def unfused():
@@ -487,6 +495,8 @@ def bench_multiply(args, torch, nb, stream):
     w = 3
     fused_ms = device_time(torch, stream, lambda: fused.run(sh), args.multiply_steps, w)
     unfused_ms = device_time(torch, stream, unfused, args.multiply_steps, w)
+    plan_ms = device_time(torch, stream, lambda: p.multiply_many(a, pb, pairs, 0, sh),
+                          args.multiply_steps, w)
     products = pairs * limbs
     words = pairs * limbs << logN
     res = {
@@ -500,6 +510,9 @@ def bench_multiply(args, torch, nb, stream):
         "unfused": {"value": products / (unfused_ms / 1000.0), "ms_per_step": unfused_ms,
                     "launches_per_step": 4, "algorithmic_bytes": 36 * words},
         "speedup_vs_unfused": unfused_ms / fused_ms,
+        "plan_fused": {"value": products / (plan_ms / 1000.0), "ms_per_step": plan_ms,
+                       "launches_per_step": 3, "algorithmic_bytes": 24 * words,
+                       "speedup_vs_unfused": unfused_ms / plan_ms},
         "kernel": {"cluster_ctas": fused.info.cluster_ctas, "clusters": fused.info.clusters,
                    "smem_bytes": fused.info.smem_bytes},
         "steps": args.multiply_steps, "warmup": w,

@@ -166,6 +166,17 @@ NTT_API ntt_status_t ntt_inverse_many(const ntt_plan_t* plan, uint32_t* a_dev, s
 NTT_API ntt_status_t ntt_pointwise_mul(const ntt_plan_t* plan, uint32_t* c_dev,
                                        const uint32_t* a_dev, const uint32_t* b_dev, size_t polys,
                                        size_t poly_stride, ntt_stream_t stream);
+/* b <- a * b, the negacyclic product per limb modulus (normal domain in and
+ * out, canonical words), for `polys` pairs (poly_stride words apart, 0 =
+ * packed; 16-byte aligned; a is read only and must not overlap b).  Three
+ * launches of the plan's transform kernels: NTT(b) in place; NTT(a) with the
+ * pointwise Montgomery product by NTT(b) folded into its store; INTT(b).  The
+ * same result as ntt_forward_many on both, ntt_pointwise_mul, then
+ * ntt_inverse_many, without the pointwise pass over HBM.  logN >= 10.  No
+ * reference counterpart (the reference has no product). */
+NTT_API ntt_status_t ntt_multiply_many(const ntt_plan_t* plan, const uint32_t* a_dev,
+                                       uint32_t* b_dev, size_t polys, size_t poly_stride,
+                                       ntt_stream_t stream);
 /* Diagnostic (no reference counterpart): 32-bit integer multiplies per second
  * the current device sustains on the transforms' multiply mix (Shoup
  * products: one multiply-high and two multiply-lows each), measured by a

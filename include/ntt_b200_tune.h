@@ -26,6 +26,9 @@ typedef struct ntt_kernel_config {
     int k2a;             /* stages of the first phase-2 register pass    */
     int threads;         /* threads per CTA                              */
     uint32_t smem_bytes; /* dynamic shared memory per CTA (direct)       */
+    int polys_per_job;   /* polynomials whose same limb one cluster
+                            transforms together, sharing every twiddle
+                            load (1, or 2 for the paired configurations) */
 } ntt_kernel_config_t;
 
 typedef struct ntt_tune_result {

@@ -86,7 +86,8 @@ class PlanInfo(ctypes.Structure):
 class KernelConfig(ctypes.Structure):
     _fields_ = [("logN", ctypes.c_int), ("cluster_ctas", ctypes.c_int), ("r1", ctypes.c_int),
                 ("words_log2", ctypes.c_int), ("k1a", ctypes.c_int), ("k2a", ctypes.c_int),
-                ("threads", ctypes.c_int), ("smem_bytes", ctypes.c_uint32)]
+                ("threads", ctypes.c_int), ("smem_bytes", ctypes.c_uint32),
+                ("polys_per_job", ctypes.c_int)]
 
 
 class TuneResult(ctypes.Structure):
@@ -146,6 +147,7 @@ _sig("ntt_inverse", _st, _vp, _vp, _vp)
 _sig("ntt_forward_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_inverse_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_pointwise_mul", _st, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
+_sig("ntt_multiply_many", _st, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_measure_int_peak", _st, ctypes.POINTER(ctypes.c_double))
 _sig("ntt_launch_ntt", _st, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_int,
      ctypes.POINTER(PhaseConfig), ctypes.POINTER(PhaseConfig))
@@ -341,6 +343,12 @@ class Plan:
         """c = a (.) b: Montgomery product of two forward outputs per limb."""
         _check(_lib.ntt_pointwise_mul(self._h, _ptr(c), _ptr(a), _ptr(b), polys, poly_stride,
                                       _stream(stream)), "ntt_pointwise_mul")
+
+    def multiply_many(self, a, b, polys: int = 1, poly_stride: int = 0, stream=None):
+        """b <- a * b negacyclic per limb (normal domain), a read only: three
+        launches, the pointwise product folded into the forward of a."""
+        _check(_lib.ntt_multiply_many(self._h, _ptr(a), _ptr(b), polys, poly_stride,
+                                      _stream(stream)), "ntt_multiply_many")
 
 
 # ---------------------------------------------------------------------------

@@ -63,18 +63,19 @@ namespace nttb {
 // first compiled configuration for logN.
 const FusedConfig* default_config(int logN, bool fwd) {
     struct Pick {
-        int logN, clog, r1, eb, k1a, k2a;
+        int logN, clog, r1, eb, k1a, k2a, np;
         bool fwd;
     };
-    static const Pick picks[] = {{16, 3, 8, 5, 3, 4, true}, {16, 3, 7, 5, 3, 5, false},
-                                 {17, 4, 8, 5, 3, 5, true}, {17, 4, 8, 5, 3, 5, false},
-                                 {15, 1, 10, 5, 5, 5, false}};
+    static const Pick picks[] = {{16, 3, 8, 5, 3, 4, 1, true}, {16, 4, 8, 4, 4, 4, 2, false},
+                                 {17, 4, 8, 5, 3, 5, 1, true}, {17, 4, 8, 5, 3, 5, 1, false},
+                                 {15, 1, 10, 5, 5, 5, 1, false}};
     const FusedConfig* c = fused_configs();
     for (const Pick& p : picks)
         if (p.logN == logN && p.fwd == fwd)
             for (int i = 0; i < fused_config_count(); ++i)
                 if (c[i].logN == p.logN && c[i].clog == p.clog && c[i].r1 == p.r1 &&
-                    c[i].eb == p.eb && c[i].k1a == p.k1a && c[i].k2a == p.k2a)
+                    c[i].eb == p.eb && c[i].k1a == p.k1a && c[i].k2a == p.k2a &&
+                    c[i].np == p.np)
                     return &c[i];
     for (int i = 0; i < fused_config_count(); ++i)
         if (c[i].logN == logN) return &c[i];
@@ -119,7 +120,9 @@ static uint32_t smem_of(const FusedConfig* c, int schedule) {
     return schedule == NTT_SCHEDULE_STAGED ? c->smem_bytes : c->smem_bytes_direct;
 }
 
-static const void* kernel_of(const FusedConfig* c, bool fwd, int schedule, bool lazy2) {
+static const void* kernel_of(const FusedConfig* c, bool fwd, int schedule, bool lazy2,
+                             bool mul = false) {
+    if (mul) return c->kern_mul[lazy2 ? 1 : 0];
     return c->kernel(schedule == NTT_SCHEDULE_STAGED, fwd, lazy2);
 }
 
@@ -191,9 +194,10 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule) {
 // wave of resident clusters, each running a contiguous chunk of limb-major
 // jobs with the next input slab bulk-copied ahead.
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
-                          int schedule, bool lazy2) {
+                          int schedule, bool lazy2, bool mul) {
     if (a.jobs == 0) return NTT_OK;
-    const void* fn = kernel_of(c, fwd, schedule, lazy2);
+    if (mul) schedule = NTT_SCHEDULE_DIRECT;  // the product epilogue has a direct form only
+    const void* fn = kernel_of(c, fwd, schedule, lazy2, mul);
     ntt_status_t st = prepare_function(c, fn, schedule);
     if (st != NTT_OK) return st;
     const unsigned C = 1u << c->clog;
@@ -546,9 +550,14 @@ namespace nttb {
 
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
-                           cudaStream_t s, uint32_t* status, int schedule, bool lazy2) {
+                           cudaStream_t s, uint32_t* status, int schedule, bool lazy2,
+                           const uint32_t* mul_src) {
     if (polys == 0) return NTT_OK;
     if (!a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL data pointer");
+    if (mul_src && (!cfg || !fwd))
+        return fail(NTT_ERR_UNSUPPORTED, "the product epilogue needs a fused forward (logN >= 10)");
+    if (mul_src && (((uintptr_t)mul_src & 15u) != 0))
+        return fail(NTT_ERR_MISALIGNED, "data must be 16-byte aligned (stride a multiple of 4 words)");
     // the fused kernels move 16-byte vectors; the small-size kernel words
     if (cfg && (((uintptr_t)a & 15u) != 0 || (polys > 1 && (stride & 3u) != 0)))
         return fail(NTT_ERR_MISALIGNED, "data must be 16-byte aligned (stride a multiple of 4 words)");
@@ -557,12 +566,15 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
     const size_t N = size_t{1} << logN;
     if (stride < (size_t)limbs * N && polys > 1)
         return fail(NTT_ERR_INVALID_ARGUMENT, "poly_stride smaller than limbs * N");
-    const size_t jobs = polys * (size_t)limbs;
-    if (jobs > (size_t)UINT_MAX) return fail(NTT_ERR_INVALID_ARGUMENT, "too many limbs");
+    // a job of the fused kernel is one limb of cfg->np polynomials
+    const size_t np = cfg ? (size_t)cfg->np : 1;
+    const size_t jobs = (polys + np - 1) / np * (size_t)limbs;
+    if (jobs > (size_t)UINT_MAX || polys > (size_t)UINT_MAX)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "too many limbs");
     if (cfg) {
         FusedArgs fa{a,  tw, q, (uint32_t)limbs, (uint32_t)polys, (uint32_t)jobs, 1u,
-                     (unsigned long long)stride, status};
-        return launch_fused(cfg, fwd, fa, s, schedule, lazy2);
+                     (unsigned long long)stride, status, mul_src, (unsigned long long)stride};
+        return launch_fused(cfg, fwd, fa, s, schedule, lazy2, mul_src != nullptr);
     }
     SmallArgs sa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride, logN};
     NTT_CUDA_TRY(launch_small(sa, fwd, s), "small NTT launch");
@@ -618,6 +630,39 @@ ntt_status_t ntt_pointwise_mul(const ntt_plan_t* p, uint32_t* c, const uint32_t*
                                   (cudaStream_t)s),
                  "pointwise launch");
     return NTT_OK;
+}
+
+ntt_status_t ntt_multiply_many(const ntt_plan_t* p, const uint32_t* a, uint32_t* b,
+                               size_t polys, size_t stride, ntt_stream_t s) {
+    if (!p || !a || !b) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!p->cfg_fwd || !p->cfg_inv)
+        return fail(NTT_ERR_UNSUPPORTED, "the fused product needs logN >= 10 (plan has %d)", p->logN);
+    if (stride == 0) stride = (size_t)p->limbs << p->logN;
+    if (polys == 0) return NTT_OK;
+    // checked before the first launch, so a refused call leaves b untouched
+    if ((((uintptr_t)a | (uintptr_t)b) & 15u) != 0 || (polys > 1 && (stride & 3u) != 0))
+        return fail(NTT_ERR_MISALIGNED, "data must be 16-byte aligned (stride a multiple of 4 words)");
+    if (polys > 1 && stride < ((size_t)p->limbs << p->logN))
+        return fail(NTT_ERR_INVALID_ARGUMENT, "poly_stride smaller than limbs * N");
+    const size_t span = ((polys - 1) * stride + ((size_t)p->limbs << p->logN)) * 4u;
+    const uintptr_t a0 = (uintptr_t)a, b0 = (uintptr_t)b;
+    if (a0 < b0 + span && b0 < a0 + span)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "the factors a and b must not overlap");
+    int dev = 0;
+    NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev != p->device)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "plan was created on device %d, current is %d",
+                    p->device, dev);
+    const cudaStream_t cs = (cudaStream_t)s;
+    // b <- NTT(b); b <- NTT(a) (.) b (product fused into the forward's store); b <- INTT(b)
+    if (ntt_status_t st = run_transform(p->logN, p->cfg_fwd, p->fwd, p->q, p->limbs, b, polys,
+                                        stride, true, cs, p->status, p->schedule, p->lazy2))
+        return st;
+    if (ntt_status_t st = run_transform(p->logN, p->cfg_fwd, p->fwd, p->q, p->limbs, b, polys,
+                                        stride, true, cs, p->status, p->schedule, p->lazy2, a))
+        return st;
+    return run_transform(p->logN, p->cfg_inv, p->inv, p->q, p->limbs, b, polys, stride, false, cs,
+                         p->status, p->schedule, p->lazy2);
 }
 
 }  // extern "C"

@@ -121,7 +121,8 @@ struct BatchCtx {
     Bcast bc;
 
     // ---- input ----
-    __device__ __forceinline__ const uint32_t* g_base(uint32_t o) const { return gin + o; }
+    // (a tile is one polynomial's limb: the polynomial index is always 0)
+    __device__ __forceinline__ const uint32_t* g_base(int, uint32_t o) const { return gin + o; }
     __device__ __forceinline__ uint32_t g_ld(const uint32_t* b, uint32_t c) const {
         if constexpr (IM == BIn::Global) return __ldca(b + c);
         else return __ldcg(b + c);
@@ -141,7 +142,7 @@ struct BatchCtx {
     __device__ __forceinline__ void st_ld4(const uint32_t*, uint32_t, uint32_t&, uint32_t&,
                                            uint32_t&, uint32_t&) const {}
     // ---- output ----
-    __device__ __forceinline__ uint32_t* o_base(uint32_t o) const { return gout + o; }
+    __device__ __forceinline__ uint32_t* o_base(int, uint32_t o) const { return gout + o; }
     __device__ __forceinline__ uint32_t mix(uint32_t v, uint32_t k) const {
         return mont_mul(v, k, q, qinv);
     }

@@ -1,6 +1,6 @@
 // Compiled fused-kernel configurations.
 //
-// X(LOGN, CLOG, R1, EB, K1A, K2A):
+// X(LOGN, CLOG, R1, EB, K1A, K2A, NP):
 //   LOGN  log2 N of the limb
 //   CLOG  log2 of the thread-block cluster size (CTAs per limb)
 //   R1    stages of phase 1 (the reference's NTT-Phase1 radix_stages); phase 2
@@ -9,35 +9,46 @@
 //         stage_merging upper bound: a pass merges up to EB radix-2 stages)
 //   K1A   stages of the first register pass of phase 1 (rest: second pass)
 //   K2A   stages of the first register pass of phase 2
-// Each logN has its own list so the instantiations compile in parallel.
+//   NP    polynomials per job: one cluster transforms the same limb of NP
+//         polynomials at once, so each twiddle it loads serves NP butterflies
+//         (2^EB words per thread per polynomial; direct schedule only)
+// Each logN has its own list so the instantiations compile in parallel
+// (logN 16 in three: two of one polynomial per job, one of two).
 #pragma once
 
-#define NTTB_CFG_N10(X) X(10, 0, 5, 5, 5, 5)
-#define NTTB_CFG_N11(X) X(11, 0, 6, 5, 1, 5)
-#define NTTB_CFG_N12(X) X(12, 0, 7, 5, 3, 5) X(12, 0, 6, 4, 3, 3)
-#define NTTB_CFG_N13(X) X(13, 0, 8, 5, 3, 5)
-#define NTTB_CFG_N14(X) X(14, 0, 9, 5, 4, 5) X(14, 1, 9, 5, 4, 5) X(14, 1, 6, 6, 6, 4)
-#define NTTB_CFG_N15(X) X(15, 1, 10, 5, 5, 5) X(15, 2, 8, 5, 3, 4) X(15, 2, 6, 6, 6, 5)
+#define NTTB_CFG_N10(X) X(10, 0, 5, 5, 5, 5, 1)
+#define NTTB_CFG_N11(X) X(11, 0, 6, 5, 1, 5, 1)
+#define NTTB_CFG_N12(X) X(12, 0, 7, 5, 3, 5, 1) X(12, 0, 6, 4, 3, 3, 1)
+#define NTTB_CFG_N13(X) X(13, 0, 8, 5, 3, 5, 1)
+#define NTTB_CFG_N14(X) X(14, 0, 9, 5, 4, 5, 1) X(14, 1, 9, 5, 4, 5, 1) X(14, 1, 6, 6, 6, 4, 1)
+#define NTTB_CFG_N15(X) X(15, 1, 10, 5, 5, 5, 1) X(15, 2, 8, 5, 3, 4, 1) X(15, 2, 6, 6, 6, 5, 1)
 #define NTTB_CFG_N16(X) \
-    X(16, 3, 8, 5, 3, 4) X(16, 3, 7, 5, 3, 5) X(16, 2, 8, 5, 3, 4) X(16, 4, 8, 5, 3, 4) \
-    X(16, 3, 8, 4, 4, 4) X(16, 3, 6, 6, 6, 5) X(16, 4, 6, 6, 6, 4)
-#define NTTB_CFG_N17(X) X(17, 3, 8, 5, 3, 5) X(17, 4, 8, 5, 3, 5) X(17, 4, 6, 6, 6, 5)
+    X(16, 3, 8, 5, 3, 4, 1) X(16, 3, 7, 5, 3, 5, 1) X(16, 2, 8, 5, 3, 4, 1) X(16, 4, 8, 5, 3, 4, 1)
+#define NTTB_CFG_N16B(X) X(16, 3, 8, 4, 4, 4, 1) X(16, 3, 6, 6, 6, 5, 1) X(16, 4, 6, 6, 6, 4, 1)
+#define NTTB_CFG_N16M(X) \
+    X(16, 3, 8, 5, 3, 4, 2) X(16, 3, 7, 5, 3, 5, 2) X(16, 4, 8, 5, 3, 4, 2) \
+    X(16, 3, 8, 4, 4, 4, 2) X(16, 4, 8, 4, 4, 4, 2)
+#define NTTB_CFG_N17(X) X(17, 3, 8, 5, 3, 5, 1) X(17, 4, 8, 5, 3, 5, 1) X(17, 4, 6, 6, 6, 5, 1)
 
 #define NTTB_CFG_ALL(X)                                                                      \
     NTTB_CFG_N10(X) NTTB_CFG_N11(X) NTTB_CFG_N12(X) NTTB_CFG_N13(X) NTTB_CFG_N14(X)      \
-    NTTB_CFG_N15(X) NTTB_CFG_N16(X) NTTB_CFG_N17(X)
+    NTTB_CFG_N15(X) NTTB_CFG_N16(X) NTTB_CFG_N16B(X) NTTB_CFG_N16M(X) NTTB_CFG_N17(X)
 
 #include <cstdint>
 
 namespace nttb {
 
 struct FusedConfig {
-    int logN, clog, r1, eb, k1a, k2a;
+    int logN, clog, r1, eb, k1a, k2a, np;
     int threads;
     uint32_t smem_bytes;         // staged kernels (work + stage buffer + mbarrier)
     uint32_t smem_bytes_direct;  // direct kernels (work buffer)
-    // fused_kernel<G, Fwd, Staged, Arith>: [staged][fwd][lazy2]
+    // fused_kernel<G, Fwd, Staged, Arith>: [staged][fwd][lazy2]; NP > 1
+    // configurations have no staged form: their staged entries are the
+    // direct kernels (run over resident chunks of jobs)
     const void* kern[2][2][2];
+    // the direct forward with the product epilogue (fused_kernel<..., Mul>): [lazy2]
+    const void* kern_mul[2];
     const void* kernel(bool staged, bool fwd, bool lazy2) const {
         return kern[staged ? 1 : 0][fwd ? 1 : 0][lazy2 ? 1 : 0];
     }

@@ -5,11 +5,21 @@
 
 namespace nttb {
 
-// Arguments of one launch over `jobs` = polys * limbs limb transforms of one
-// plan.  Jobs are numbered limb-major (job j: limb j / polys, polynomial
-// j % polys) so that consecutive jobs share a modulus and its twiddles;
-// cluster c runs jobs [c * jobs_per_cluster, (c+1) * jobs_per_cluster).
+// Arguments of one launch over the limb transforms of `polys` polynomials of
+// `limbs` limbs of one plan.  A job is one limb of NP polynomials (the
+// kernel's G::NP; the NP transforms share every twiddle load): `jobs` =
+// limbs * ceil(polys / NP), numbered limb-major (job j: limb j / groups,
+// polynomials NP * (j % groups) + 0..NP-1, groups = ceil(polys / NP)) so that
+// consecutive jobs share a modulus and its twiddles.  When NP does not divide
+// polys, the last group repeats the last polynomial (the same words computed
+// twice and stored twice: every read of a limb precedes the cluster barrier
+// that precedes every write of it).  Cluster c runs jobs
+// [c * jobs_per_cluster, (c+1) * jobs_per_cluster).
 // Polynomial p starts at data + p * poly_stride (words), limb l at + l * N.
+// The forward kernel with the product epilogue (Mul) reads its input from
+// src (polynomial p at src + p * src_stride) and stores the Montgomery
+// product of each output word with the word at the same place of `data`
+// (a spectrum) into that place.
 struct FusedArgs {
     uint32_t* data;
     const TwPair* tw;   // [limbs][N] forward or inverse table (see twiddle.cu)
@@ -20,7 +30,31 @@ struct FusedArgs {
     uint32_t jobs_per_cluster;
     unsigned long long poly_stride;
     uint32_t* status;  // optional: bit 0 set when a bounded wait expired
+    const uint32_t* src;  // Mul only: the forward's input
+    unsigned long long src_stride;
 };
+
+// -q^{-1} mod 2^32 by Newton's iteration (q odd: q is its own inverse mod 8).
+__device__ __forceinline__ uint32_t neg_qinv_dev(uint32_t q) {
+    uint32_t x = q;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) x *= 2u - q * x;
+    return 0u - x;
+}
+
+// Output base of the product epilogue: the spectrum it multiplies by sits
+// at the same place as the product it stores.  A job slot that repeats the
+// last polynomial (NP not dividing polys) stores nothing (live == false): a
+// second read-modify-write of the same words would multiply twice.
+struct MulOut {
+    uint32_t* p;
+    bool live;
+};
+
+// Hint: fetch [src, src + bytes) from HBM into L2 (no completion tracking).
+__device__ __forceinline__ void prefetch_l2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
 
 // Iteration bound of every mbarrier wait (each try_wait itself blocks for a
 // hardware-defined interval); expiry sets the status bit instead of hanging.
@@ -84,10 +118,13 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst_sa, const void* src, uint3
 // Memory interface used by the pass code (ntt_core.cuh): every access is a
 // per-thread base plus a compile-time offset, which the compiler turns into
 // an immediate address offset.
-template <int C, bool Staged>
+template <int C, bool Staged, int NP, bool Mul = false>
 struct DevCtx {
     static constexpr bool kStaged = Staged;
-    uint32_t* __restrict__ g;
+    uint32_t* g[NP];  // limb base of each polynomial of the job (input)
+    uint32_t* o[NP];  // ... output (the input's place, or the spectrum for Mul)
+    uint32_t qinv;    // Mul: -q^{-1} mod 2^32
+    uint32_t live;    // Mul: bit p set when slot p is not a repeated polynomial
     const TwPair* __restrict__ twp;
     uint32_t* smem;
     const uint32_t* stage;  // padded copy of this CTA's input slab (staged)
@@ -96,7 +133,7 @@ struct DevCtx {
 
     // global data (direct input): L1-cached, because a thread owning a
     // contiguous run reads each 32-byte sector in two 16-byte halves
-    __device__ __forceinline__ uint32_t* g_base(uint32_t o) const { return g + o; }
+    __device__ __forceinline__ uint32_t* g_base(int p, uint32_t o) const { return g[p] + o; }
     __device__ __forceinline__ uint32_t g_ld(const uint32_t* b, uint32_t c) const {
         return __ldca(b + c);
     }
@@ -108,12 +145,28 @@ struct DevCtx {
         z = t.z;
         w = t.w;
     }
-    // transform output: in place
-    __device__ __forceinline__ uint32_t* o_base(uint32_t o) const { return g + o; }
+    // transform output: in place, or (Mul) the product with the spectrum
+    // word at the output's place (written by an earlier launch: read via L2)
+    __device__ __forceinline__ auto o_base(int p, uint32_t off) const {
+        if constexpr (Mul) return MulOut{o[p] + off, ((live >> p) & 1u) != 0};
+        else return o[p] + off;
+    }
     __device__ __forceinline__ void o_st(uint32_t* b, uint32_t c, uint32_t v) const { b[c] = v; }
     __device__ __forceinline__ void o_st4(uint32_t* b, uint32_t c, uint32_t x, uint32_t y,
                                           uint32_t z, uint32_t w) const {
         *reinterpret_cast<uint4*>(b + c) = make_uint4(x, y, z, w);
+    }
+    __device__ __forceinline__ void o_st(MulOut b, uint32_t c, uint32_t v) const {
+        if (!b.live) return;
+        b.p[c] = mont_mul(v, __ldcg(b.p + c), q, qinv);
+    }
+    __device__ __forceinline__ void o_st4(MulOut b, uint32_t c, uint32_t x, uint32_t y,
+                                          uint32_t z, uint32_t w) const {
+        if (!b.live) return;
+        const uint4 k = __ldcg(reinterpret_cast<const uint4*>(b.p + c));
+        *reinterpret_cast<uint4*>(b.p + c) =
+            make_uint4(mont_mul(x, k.x, q, qinv), mont_mul(y, k.y, q, qinv),
+                       mont_mul(z, k.z, q, qinv), mont_mul(w, k.w, q, qinv));
     }
     // stage buffer
     __device__ __forceinline__ const uint32_t* st_base(uint32_t w) const { return stage + w; }
@@ -253,8 +306,10 @@ __device__ __forceinline__ void fused_inverse_body(Ctx& ctx, Pre&& prefetch) {
 // Arith: the range discipline of every limb of the launch (Lazy4 needs all
 // moduli below 2^30; Lazy2 takes any below 2^31), fixed per kernel so that
 // one path's registers fit the launch bounds.
-template <class G, bool Fwd, bool Staged, class Arith>
+// Mul (forward, direct only): the product epilogue of FusedArgs.
+template <class G, bool Fwd, bool Staged, class Arith, bool Mul = false>
 __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedArgs a) {
+    static_assert(!Mul || (Fwd && !Staged), "the product epilogue follows a direct forward");
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t rank = (G::C > 1) ? cluster_rank() : 0u;
     const uint32_t cluster = blockIdx.x / G::C;
@@ -271,18 +326,36 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedA
         __syncthreads();
         if (j0 < j1) issue_slab<G, Fwd>(a, j0, rank, stage_sa, mbar_sa);
     }
-    DevCtx<G::C, Staged> ctx;
+    static_assert(!Staged || G::NP == 1, "the staged schedule carries one polynomial per job");
+    DevCtx<G::C, Staged, G::NP, Mul> ctx;
+    const uint32_t groups = (a.polys + G::NP - 1) / G::NP;
     ctx.smem = smem;
     ctx.stage = smem + G::STAGE_OFF_WORDS;
     ctx.smem_sa = smem_sa;
     ctx.rank = rank;
     uint32_t parity = 0;
     for (uint32_t job = j0; job < j1; ++job, parity ^= 1u) {
-        const uint32_t limb = job / a.polys, poly = job - limb * a.polys;
-        ctx.g = a.data + (size_t)poly * a.poly_stride + ((size_t)limb << G::LOGN);
+        const uint32_t limb = job / groups, poly0 = (job - limb * groups) * G::NP;
+        if constexpr (Mul) ctx.live = 0;
+#pragma unroll
+        for (int p = 0; p < G::NP; ++p) {
+            const size_t poly = min(poly0 + p, a.polys - 1);
+            ctx.o[p] = a.data + poly * a.poly_stride + ((size_t)limb << G::LOGN);
+            if constexpr (Mul) {
+                ctx.g[p] = const_cast<uint32_t*>(a.src) + poly * a.src_stride +
+                           ((size_t)limb << G::LOGN);
+                if (poly0 + p < a.polys) ctx.live |= 1u << p;
+                // the spectrum words this CTA multiplies by at the end (its
+                // phase-2 slab): start moving them into L2 now
+                if (threadIdx.x == 0) prefetch_l2(ctx.o[p] + rank * G::M, G::M * 4u);
+            } else {
+                ctx.g[p] = ctx.o[p];
+            }
+        }
         ctx.twp = a.tw + ((size_t)limb << G::LOGN);
         ctx.q = __ldg(a.q + limb);
         ctx.q2 = 2u * ctx.q;
+        if constexpr (Mul) ctx.qinv = neg_qinv_dev(ctx.q);
         if constexpr (Staged) {
             if (!mbar_wait_bounded(mbar_sa, parity) && a.status)
                 atomicOr(a.status, kStatusWaitExpired);

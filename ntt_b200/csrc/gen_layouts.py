@@ -25,9 +25,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def configs():
+    """Distinct (N, CL, R1, EB, K1A, K2A) of configs.h: the layout of a slab
+    does not depend on the polynomials per job (NP, the 7th field)."""
     src = open(os.path.join(HERE, "configs.h")).read().split("#define NTTB_CFG_ALL")[0]
-    return [tuple(int(v) for v in m) for m in
-            re.findall(r"X\((\d+), (\d+), (\d+), (\d+), (\d+), (\d+)\)", src)]
+    out = []
+    for m in re.findall(r"X\((\d+), (\d+), (\d+), (\d+), (\d+), (\d+), (\d+)\)", src):
+        g = tuple(int(v) for v in m[:6])
+        if g not in out:
+            out.append(g)
+    return out
 
 
 def pass_lanes(MB, PLO, KB, EB, WM):

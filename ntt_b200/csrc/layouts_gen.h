@@ -173,6 +173,15 @@ struct LayoutTable<16, 4, 6, 6, 6, 4> {
 };
 
 template <>
+struct LayoutTable<16, 4, 8, 4, 4, 4> {
+    static constexpr int XW[5] = {5, 1, 8, 8, 4343};
+    static constexpr uint32_t lanes_P1A = 0x1fu;
+    static constexpr uint32_t lanes_P1B = 0x10fu;
+    static constexpr uint32_t lanes_P2A = 0x10fu;
+    static constexpr uint32_t lanes_P2B = 0x1f0u;
+};
+
+template <>
 struct LayoutTable<17, 3, 8, 5, 3, 5> {
     static constexpr int XW[5] = {5, 1, 14, 0, 16895};
     static constexpr uint32_t lanes_P1A = 0x7cu;

@@ -184,9 +184,10 @@ struct StageLayout {
 //   EB: log2 words per thread per pass;  K1A / K2A: stages of the first
 //   register pass of phase 1 / phase 2 (the rest, if any, is a second pass).
 // ---------------------------------------------------------------------------
-template <int LOGN_, int CLOG_, int R1_, int EB_, int K1A_, int K2A_>
+template <int LOGN_, int CLOG_, int R1_, int EB_, int K1A_, int K2A_, int NP_ = 1>
 struct Geometry {
     static constexpr int LOGN = LOGN_, CLOG = CLOG_, R1 = R1_, EB = EB_;
+    static constexpr int NP = NP_;  // polynomials per job (same limb, same twiddles)
     static constexpr int R2 = LOGN - R1;
     static constexpr int C = 1 << CLOG;
     static constexpr int MB = LOGN - CLOG;  // local bits
@@ -199,9 +200,13 @@ struct Geometry {
     // Register budget: the transforms are latency-bound and gain more from
     // resident warps than from per-thread ILP (measured on B200: 5 CTAs of
     // 256 threads at 48 registers beat 4 at 64 and 3 at 85), so ask for as
-    // many resident CTAs as leave each thread its 2^EB data words plus 16
-    // registers, and at least 40.
-    static constexpr int REG_BUDGET = (1 << EB_) + 16 > 40 ? (1 << EB_) + 16 : 40;
+    // many resident CTAs as leave each thread its NP * 2^EB data words plus
+    // 16 registers, and at least 40.
+    // (24 spare registers with several polynomials per job: each keeps a
+    // global base pointer of its own, and 16 spare registers spilled)
+    static constexpr int REG_SPARE = NP > 1 ? 24 : 16;
+    static constexpr int REG_BUDGET =
+        NP * (1 << EB_) + REG_SPARE > 40 ? NP * (1 << EB_) + REG_SPARE : 40;
     static constexpr int MIN_BLOCKS =
         (65536 / (THREADS * REG_BUDGET)) > 0 ? (65536 / (THREADS * REG_BUDGET)) : 1;
     static constexpr int K1A = K1A_, K1B = R1 - K1A_;
@@ -245,7 +250,9 @@ struct Geometry {
                       LT::lanes_P2A == P2A::kLanes && LT::lanes_P2B == P2B::kLanes,
                   "layouts_gen.h is stale: rerun gen_layouts.py");
     using XW = Spread<LT::XW[0], LT::XW[1], LT::XW[2], LT::XW[3]>;
-    static constexpr uint32_t SMEM_WORDS = ((uint32_t)LT::XW[4] + 3u) & ~3u;
+    // one slab of the layout per polynomial of the job
+    static constexpr uint32_t SLAB_WORDS = ((uint32_t)LT::XW[4] + 3u) & ~3u;
+    static constexpr uint32_t SMEM_WORDS = NP * SLAB_WORDS;
     // dynamic shared memory: work buffer | stage buffer | mbarrier
     static constexpr uint32_t STAGE_OFF_WORDS = SMEM_WORDS;
     static constexpr uint32_t MBAR_OFF_WORDS = (STAGE_OFF_WORDS + STAGE_WORDS + 3u) & ~3u;
@@ -314,8 +321,10 @@ struct Maps {
 // top KB-1-k butterfly bits.  `tbase` is the twiddle index of group 0 for
 // this thread; group g of extra-high coordinate xh uses tbase + xoff(xh) + g.
 // Fold: the limb's stage 0 (one twiddle, index 1) with the factor in entry 0.
-template <class L, class Arith, bool Fwd, int k, bool Fold, class Ctx>
-NTT_HD void stage(Ctx& ctx, uint32_t (&v)[L::E], uint32_t tbase) {
+// v[p][r]: register r of polynomial p; every twiddle loaded once serves the
+// same butterfly of all NP polynomials of the job.
+template <class L, class Arith, bool Fwd, int k, bool Fold, int NP, class Ctx>
+NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
     constexpr int p = Fwd ? (L::PLO + L::KB - 1 - k) : (L::PLO + k);
     constexpr int gbits = Fwd ? k : (L::KB - 1 - k);
     constexpr int bbit = Fwd ? (L::KB - 1 - k) : k;  // butterfly coordinate bit
@@ -330,8 +339,11 @@ NTT_HD void stage(Ctx& ctx, uint32_t (&v)[L::E], uint32_t tbase) {
             constexpr int i = decltype(I)::value;
             // the E/2 pairs: the lower register has bit (bbit + XB) clear
             constexpr int r = ((i >> (bbit + L::XB)) << (bbit + L::XB + 1)) | (i & (stride - 1));
-            if constexpr (Fwd) Arith::ct_first(v[r], v[r + stride], f, w, q, q2);
-            else Arith::gs_last(v[r], v[r + stride], f, w, q, q2);
+            ct_for<NP>([&](auto Pp) {
+                constexpr int pp = decltype(Pp)::value;
+                if constexpr (Fwd) Arith::ct_first(v[pp][r], v[pp][r + stride], f, w, q, q2);
+                else Arith::gs_last(v[pp][r], v[pp][r + stride], f, w, q, q2);
+            });
         });
     } else {
         ct_for<(1 << XHB)>([&](auto XH) {
@@ -356,8 +368,13 @@ NTT_HD void stage(Ctx& ctx, uint32_t (&v)[L::E], uint32_t tbase) {
                         constexpr int xl = decltype(XL)::value;
                         constexpr int bc = (g << (bbit + 1)) | lo;
                         constexpr int r = (bc << L::XB) | (xh << XLB) | xl;
-                        if constexpr (Fwd) Arith::ct(v[r], v[r + stride], w[g].w, w[g].wp, q, q2);
-                        else Arith::gs(v[r], v[r + stride], w[g].w, w[g].wp, q, q2);
+                        ct_for<NP>([&](auto Pp) {
+                            constexpr int pp = decltype(Pp)::value;
+                            if constexpr (Fwd)
+                                Arith::ct(v[pp][r], v[pp][r + stride], w[g].w, w[g].wp, q, q2);
+                            else
+                                Arith::gs(v[pp][r], v[pp][r + stride], w[g].w, w[g].wp, q, q2);
+                        });
                     });
                 });
             });
@@ -373,7 +390,7 @@ NTT_HD void stage(Ctx& ctx, uint32_t (&v)[L::E], uint32_t tbase) {
 // memory -- so the wait before the scatter overlaps the remaining stages.
 template <class G, class L, class Arith, bool Fwd, bool Phase2, bool HasStage0,
           bool ArriveAfterFirst = false, class Ctx>
-NTT_HD void run_stages(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
+NTT_HD void run_stages(Ctx& ctx, uint32_t (&v)[G::NP][L::E], uint32_t d) {
     using Mp = Maps<G>;
     ct_for<L::KB>([&](auto K) {
         constexpr int k = decltype(K)::value;
@@ -381,7 +398,7 @@ NTT_HD void run_stages(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
         constexpr bool s0 = HasStage0 && (Fwd ? (k == 0) : (k == L::KB - 1));
         const uint32_t tb =
             (Phase2 ? Mp::tw_base_p2(p, ctx.rank) : Mp::tw_base_p1(p)) + (d >> (p + 1));
-        stage<L, Arith, Fwd, k, s0>(ctx, v, tb);
+        stage<L, Arith, Fwd, k, s0, G::NP>(ctx, v, tb);
         if constexpr (ArriveAfterFirst && k == 0) ctx.after_local_reads();
     });
 }
@@ -398,94 +415,110 @@ constexpr bool use_vec4() {
     return L::kRunBits >= 2 && Lim >= 4;
 }
 
-// GMap::map(o): word offset of register offset o (linear, no base term)
-template <class L, uint32_t Lim, class GMap, class Ctx>
-NTT_HD void load_global(Ctx& ctx, uint32_t (&v)[L::E], uint32_t gbase) {
-    auto gb = ctx.g_base(gbase);
-    if constexpr (use_vec4<L, Lim>()) {
-        ct_for<L::E>([&](auto R) {
-            constexpr int r = decltype(R)::value;
-            constexpr uint32_t o = L::off(r);
-            if constexpr ((o & 3u) == 0) {
-                ctx.g_ld4(gb, GMap::map(o), v[L::reg_of(o)], v[L::reg_of(o + 1)],
-                          v[L::reg_of(o + 2)], v[L::reg_of(o + 3)]);
-            }
-        });
-    } else {
-        ct_for<L::E>([&](auto R) {
-            constexpr int r = decltype(R)::value;
-            v[r] = ctx.g_ld(gb, GMap::map(L::off(r)));
-        });
-    }
+// GMap::map(o): word offset of register offset o (linear, no base term).
+// Polynomial p of the job has its own global base (ctx.g_base(p, ...)).
+template <class L, uint32_t Lim, class GMap, int NP, class Ctx>
+NTT_HD void load_global(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t gbase) {
+    ct_for<NP>([&](auto Pp) {
+        constexpr int pp = decltype(Pp)::value;
+        auto gb = ctx.g_base(pp, gbase);
+        if constexpr (use_vec4<L, Lim>()) {
+            ct_for<L::E>([&](auto R) {
+                constexpr int r = decltype(R)::value;
+                constexpr uint32_t o = L::off(r);
+                if constexpr ((o & 3u) == 0) {
+                    ctx.g_ld4(gb, GMap::map(o), v[pp][L::reg_of(o)], v[pp][L::reg_of(o + 1)],
+                              v[pp][L::reg_of(o + 2)], v[pp][L::reg_of(o + 3)]);
+                }
+            });
+        } else {
+            ct_for<L::E>([&](auto R) {
+                constexpr int r = decltype(R)::value;
+                v[pp][r] = ctx.g_ld(gb, GMap::map(L::off(r)));
+            });
+        }
+    });
 }
 
 // The transform's output goes through the context's o_* interface (global
 // memory for a plain transform; a fused caller may redirect it).
-template <class L, uint32_t Lim, class GMap, class Ctx, class ValFn>
-NTT_HD void store_global(Ctx& ctx, uint32_t (&v)[L::E], uint32_t gbase, ValFn fin) {
-    auto gb = ctx.o_base(gbase);
-    if constexpr (use_vec4<L, Lim>()) {
-        ct_for<L::E>([&](auto R) {
-            constexpr int r = decltype(R)::value;
-            constexpr uint32_t o = L::off(r);
-            if constexpr ((o & 3u) == 0) {
-                ctx.o_st4(gb, GMap::map(o), fin(v[L::reg_of(o)]), fin(v[L::reg_of(o + 1)]),
-                          fin(v[L::reg_of(o + 2)]), fin(v[L::reg_of(o + 3)]));
-            }
-        });
-    } else {
-        ct_for<L::E>([&](auto R) {
-            constexpr int r = decltype(R)::value;
-            ctx.o_st(gb, GMap::map(L::off(r)), fin(v[r]));
-        });
-    }
+template <class L, uint32_t Lim, class GMap, int NP, class Ctx, class ValFn>
+NTT_HD void store_global(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t gbase, ValFn fin) {
+    ct_for<NP>([&](auto Pp) {
+        constexpr int pp = decltype(Pp)::value;
+        auto gb = ctx.o_base(pp, gbase);
+        if constexpr (use_vec4<L, Lim>()) {
+            ct_for<L::E>([&](auto R) {
+                constexpr int r = decltype(R)::value;
+                constexpr uint32_t o = L::off(r);
+                if constexpr ((o & 3u) == 0) {
+                    ctx.o_st4(gb, GMap::map(o), fin(v[pp][L::reg_of(o)]),
+                              fin(v[pp][L::reg_of(o + 1)]), fin(v[pp][L::reg_of(o + 2)]),
+                              fin(v[pp][L::reg_of(o + 3)]));
+                }
+            });
+        } else {
+            ct_for<L::E>([&](auto R) {
+                constexpr int r = decltype(R)::value;
+                ctx.o_st(gb, GMap::map(L::off(r)), fin(v[pp][r]));
+            });
+        }
+    });
 }
 
-// Stage buffer (the bulk-copied input slab).
-template <class L, class Ctx>
-NTT_HD void load_stage(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
+// Stage buffer (the bulk-copied input slab; one polynomial per job).
+template <class L, int NP, class Ctx>
+NTT_HD void load_stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t d) {
+    static_assert(NP == 1, "the staged schedule carries one polynomial per job");
     auto sb = ctx.st_base(StageLayout::phys(d));
     if constexpr (L::kRunBits >= 2) {
         ct_for<L::E>([&](auto R) {
             constexpr int r = decltype(R)::value;
             constexpr uint32_t o = L::off(r);
             if constexpr ((o & 3u) == 0)
-                ctx.st_ld4(sb, StageLayout::phys(o), v[L::reg_of(o)], v[L::reg_of(o + 1)],
-                           v[L::reg_of(o + 2)], v[L::reg_of(o + 3)]);
+                ctx.st_ld4(sb, StageLayout::phys(o), v[0][L::reg_of(o)], v[0][L::reg_of(o + 1)],
+                           v[0][L::reg_of(o + 2)], v[0][L::reg_of(o + 3)]);
         });
     } else {
         ct_for<L::E>([&](auto R) {
             constexpr int r = decltype(R)::value;
-            v[r] = ctx.st_ld(sb, StageLayout::phys(L::off(r)));
+            v[0][r] = ctx.st_ld(sb, StageLayout::phys(L::off(r)));
         });
     }
 }
 
 // The input slab of a transform: from the stage buffer (bulk-copied ahead of
 // time) or straight from global memory, as the context's kStaged says.
-template <class L, uint32_t Lim, class GMap, class Ctx>
-NTT_HD void load_input(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d, uint32_t gbase) {
+template <class L, uint32_t Lim, class GMap, int NP, class Ctx>
+NTT_HD void load_input(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t d, uint32_t gbase) {
     if constexpr (Ctx::kStaged)
         load_stage<L>(ctx, v, d);
     else
         load_global<L, Lim, GMap>(ctx, v, gbase);
 }
 
-template <class L, class X, class Ctx>
-NTT_HD void load_smem(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
+// Work buffer: polynomial p's slab starts Slab words after polynomial 0's.
+template <class L, class X, uint32_t Slab, int NP, class Ctx>
+NTT_HD void load_smem(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t d) {
     auto sb = ctx.s_base(X::phys(d));
     ct_for<L::E>([&](auto R) {
         constexpr int r = decltype(R)::value;
-        v[r] = ctx.s_ld(sb, X::phys(L::off(r)));
+        ct_for<NP>([&](auto Pp) {
+            constexpr int pp = decltype(Pp)::value;
+            v[pp][r] = ctx.s_ld(sb, pp * Slab + X::phys(L::off(r)));
+        });
     });
 }
 
-template <class L, class X, class Ctx>
-NTT_HD void store_smem(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
+template <class L, class X, uint32_t Slab, int NP, class Ctx>
+NTT_HD void store_smem(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t d) {
     auto sb = ctx.s_base(X::phys(d));
     ct_for<L::E>([&](auto R) {
         constexpr int r = decltype(R)::value;
-        ctx.s_st(sb, X::phys(L::off(r)), v[r]);
+        ct_for<NP>([&](auto Pp) {
+            constexpr int pp = decltype(Pp)::value;
+            ctx.s_st(sb, pp * Slab + X::phys(L::off(r)), v[pp][r]);
+        });
     });
 }
 
@@ -539,13 +572,16 @@ struct ILam {
 
 // Scatter one pass's registers to their owners' shared memory (DSMEM when
 // C > 1).  The destination word is phys(base) + phys(map(offset)).
-template <class L, class X, class Ctx, class DstF, class LamF>
-NTT_HD void scatter_regs(Ctx& ctx, uint32_t (&v)[L::E], uint32_t dd, uint32_t dl) {
+template <class L, class X, uint32_t Slab, int NP, class Ctx, class DstF, class LamF>
+NTT_HD void scatter_regs(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t dd, uint32_t dl) {
     ct_for<L::E>([&](auto R) {
         constexpr int r = decltype(R)::value;
         constexpr uint32_t o = L::off(r);
         auto rb = ctx.r_base(dd + DstF::map(o), X::phys(dl));
-        ctx.template r_st<X::phys(LamF::map(o))>(rb, v[r]);
+        ct_for<NP>([&](auto Pp) {
+            constexpr int pp = decltype(Pp)::value;
+            ctx.template r_st<pp * Slab + X::phys(LamF::map(o))>(rb, v[pp][r]);
+        });
     });
 }
 
@@ -559,20 +595,20 @@ struct Forward {
     using P2B = typename G::P2B;
 
     template <class L>
-    NTT_HD static void scatter(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
-        scatter_regs<L, X, Ctx, FDst<G>, FLam<G>>(ctx, v, Mp::f_dst(d),
+    NTT_HD static void scatter(Ctx& ctx, uint32_t (&v)[G::NP][L::E], uint32_t d) {
+        scatter_regs<L, X, G::SLAB_WORDS, G::NP, Ctx, FDst<G>, FLam<G>>(ctx, v, Mp::f_dst(d),
                                                  Mp::f_lam(d) + Mp::g1_rank(ctx.rank));
     }
 
     // Phase-1 first pass: input slab (normal domain) -> stages incl. stage 0
     // -> work buffer (if a second phase-1 pass follows) or the scatter.
     NTT_HD static void pass1a(Ctx& ctx, uint32_t tid) {
-        uint32_t v[P1A::E];
+        uint32_t v[G::NP][P1A::E];
         const uint32_t d = P1A::dep(tid);
         load_input<P1A, G::W1, G1Map<G>>(ctx, v, d, Mp::g1(d) + Mp::g1_rank(ctx.rank));
         run_stages<G, P1A, Arith, true, false, true, (G::K1B == 0)>(ctx, v, d);
         if constexpr (G::K1B > 0) {
-            store_smem<P1A, X>(ctx, v, d);
+            store_smem<P1A, X, G::SLAB_WORDS>(ctx, v, d);
         } else {
             ctx.before_scatter();
             scatter<P1A>(ctx, v, d);
@@ -580,21 +616,21 @@ struct Forward {
     }
     NTT_HD static void pass1b(Ctx& ctx, uint32_t tid) {
         if constexpr (G::K1B > 0) {
-            uint32_t v[P1B::E];
+            uint32_t v[G::NP][P1B::E];
             const uint32_t d = P1B::dep(tid);
-            load_smem<P1B, X>(ctx, v, d);
+            load_smem<P1B, X, G::SLAB_WORDS>(ctx, v, d);
             run_stages<G, P1B, Arith, true, false, false, true>(ctx, v, d);
             ctx.before_scatter();
             scatter<P1B>(ctx, v, d);
         }
     }
     NTT_HD static void pass2a(Ctx& ctx, uint32_t tid) {
-        uint32_t v[P2A::E];
+        uint32_t v[G::NP][P2A::E];
         const uint32_t d = P2A::dep(tid);
-        load_smem<P2A, X>(ctx, v, d);
+        load_smem<P2A, X, G::SLAB_WORDS>(ctx, v, d);
         run_stages<G, P2A, Arith, true, true, false>(ctx, v, d);
         if constexpr (G::K2B > 0) {
-            store_smem<P2A, X>(ctx, v, d);
+            store_smem<P2A, X, G::SLAB_WORDS>(ctx, v, d);
         } else {
             store_global<P2A, (1u << 30), G2Map>(ctx, v, d + ctx.rank * G::M,
                                                  FwdFinal<Arith>{ctx.q, ctx.q2});
@@ -602,9 +638,9 @@ struct Forward {
     }
     NTT_HD static void pass2b(Ctx& ctx, uint32_t tid) {
         if constexpr (G::K2B > 0) {
-            uint32_t v[P2B::E];
+            uint32_t v[G::NP][P2B::E];
             const uint32_t d = P2B::dep(tid);
-            load_smem<P2B, X>(ctx, v, d);
+            load_smem<P2B, X, G::SLAB_WORDS>(ctx, v, d);
             run_stages<G, P2B, Arith, true, true, false>(ctx, v, d);
             store_global<P2B, (1u << 30), G2Map>(ctx, v, d + ctx.rank * G::M,
                                                  FwdFinal<Arith>{ctx.q, ctx.q2});
@@ -622,8 +658,8 @@ struct Inverse {
     using P2B = typename G::P2B;
 
     template <class L>
-    NTT_HD static void scatter(Ctx& ctx, uint32_t (&v)[L::E], uint32_t d) {
-        scatter_regs<L, X, Ctx, IDst<G>, ILam<G>>(ctx, v, Mp::i_dst(d),
+    NTT_HD static void scatter(Ctx& ctx, uint32_t (&v)[G::NP][L::E], uint32_t d) {
+        scatter_regs<L, X, G::SLAB_WORDS, G::NP, Ctx, IDst<G>, ILam<G>>(ctx, v, Mp::i_dst(d),
                                                  Mp::i_lam(d) + Mp::i_lam_rank(ctx.rank));
     }
 
@@ -631,18 +667,18 @@ struct Inverse {
     // The first pass reads the contiguous phase-2 slab (stage or global).
     template <class L, bool Last, bool FromInput>
     NTT_HD static void phase2_pass(Ctx& ctx, uint32_t tid) {
-        uint32_t v[L::E];
+        uint32_t v[G::NP][L::E];
         const uint32_t d = L::dep(tid);
         if constexpr (FromInput)
             load_input<L, (1u << 30), G2Map>(ctx, v, d, d + ctx.rank * G::M);
         else
-            load_smem<L, X>(ctx, v, d);
+            load_smem<L, X, G::SLAB_WORDS>(ctx, v, d);
         run_stages<G, L, Arith, false, true, false, Last>(ctx, v, d);
         if constexpr (Last) {
             ctx.before_scatter();
             scatter<L>(ctx, v, d);
         } else {
-            store_smem<L, X>(ctx, v, d);
+            store_smem<L, X, G::SLAB_WORDS>(ctx, v, d);
         }
     }
     NTT_HD static void pass2b(Ctx& ctx, uint32_t tid) {
@@ -653,19 +689,19 @@ struct Inverse {
     }
     NTT_HD static void pass1b(Ctx& ctx, uint32_t tid) {
         if constexpr (G::K1B > 0) {
-            uint32_t v[P1B::E];
+            uint32_t v[G::NP][P1B::E];
             const uint32_t d = P1B::dep(tid);
-            load_smem<P1B, X>(ctx, v, d);
+            load_smem<P1B, X, G::SLAB_WORDS>(ctx, v, d);
             run_stages<G, P1B, Arith, false, false, false>(ctx, v, d);
-            store_smem<P1B, X>(ctx, v, d);
+            store_smem<P1B, X, G::SLAB_WORDS>(ctx, v, d);
         }
     }
     // Last pass: contains the limb's stage 0 (fold N^{-1} R^{-1}), canonical
     // output to the phase-1 slab in global memory.
     NTT_HD static void pass1a(Ctx& ctx, uint32_t tid) {
-        uint32_t v[P1A::E];
+        uint32_t v[G::NP][P1A::E];
         const uint32_t d = P1A::dep(tid);
-        load_smem<P1A, X>(ctx, v, d);
+        load_smem<P1A, X, G::SLAB_WORDS>(ctx, v, d);
         run_stages<G, P1A, Arith, false, false, true>(ctx, v, d);
         store_global<P1A, G::W1, G1Map<G>>(ctx, v, Mp::g1(d) + Mp::g1_rank(ctx.rank), Ident{});
     }

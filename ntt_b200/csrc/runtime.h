@@ -24,16 +24,21 @@ const FusedConfig* tuned_config(int logN, int limbs, bool fwd);
 int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule);
 // One launch of a fused configuration under a schedule (NTT_SCHEDULE_*);
 // lazy2: some modulus is >= 2^30 (the [0, 2q) range discipline for all).
+// mul: the direct forward with the product epilogue (FusedArgs.src).
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
-                          int schedule, bool lazy2);
+                          int schedule, bool lazy2, bool mul = false);
 ntt_status_t validate_modulus(int logN, ModulusConfig m, ModulusRuntime* rt);
 // Validates m and fills the twiddle-generation inputs of both directions
 // (entries 0/1 carry the folded Montgomery / N^{-1} R^{-1} factors).
 ntt_status_t twiddle_gen_inputs(int logN, ModulusConfig m, TwGenLimb* fwd, TwGenLimb* inv);
 // One launch over `polys` polynomials of `limbs` limbs (cfg == nullptr: the
 // single-CTA small-size kernel).  status: optional device error word.
+// mul_src (fused forward only): transform mul_src (same shape and stride)
+// instead and store the Montgomery product of each output word with the
+// spectrum word already at its place in `a`.
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
-                           cudaStream_t s, uint32_t* status, int schedule, bool lazy2);
+                           cudaStream_t s, uint32_t* status, int schedule, bool lazy2,
+                           const uint32_t* mul_src = nullptr);
 
 }  // namespace nttb

@@ -117,8 +117,9 @@ int ntt_config_count(void) { return fused_config_count(); }
 ntt_status_t ntt_config_get(int index, ntt_kernel_config_t* out) {
     const FusedConfig* c = config_by_index(index);
     if (!c || !out) return fail(NTT_ERR_INVALID_ARGUMENT, "bad config index %d", index);
-    *out = ntt_kernel_config_t{c->logN, 1 << c->clog, c->r1,     c->eb,
-                               c->k1a,  c->k2a,       c->threads, c->smem_bytes_direct};
+    *out = ntt_kernel_config_t{c->logN, 1 << c->clog, c->r1,      c->eb,
+                               c->k1a,  c->k2a,       c->threads, c->smem_bytes_direct,
+                               c->np};
     return NTT_OK;
 }
 

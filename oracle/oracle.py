@@ -114,6 +114,9 @@ def ref_lib() -> Optional[ctypes.CDLL]:
         for n in ("ref_gpu_launch_ntt16", "ref_gpu_launch_intt16"):
             getattr(R, n).restype = ctypes.c_int
             getattr(R, n).argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_size_t]
+        R.ref_gpu_time16.restype = ctypes.c_int
+        R.ref_gpu_time16.argtypes = ([ctypes.c_void_p] * 8 + [ctypes.c_size_t, ctypes.c_int,
+                                     ctypes.c_int] + [ctypes.POINTER(ctypes.c_float)] * 2)
         _REF = R
     return _REF
 

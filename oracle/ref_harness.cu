@@ -86,4 +86,44 @@ int ref_gpu_launch_intt16(uint32_t* A, const uint32_t* itw, const uint32_t* modu
     return (int)cudaDeviceSynchronize();
 }
 
+// Device time (CUDA events, legacy default stream, as v04:980-998) of the
+// reference's per-call path at logN = 16 over `polys` packed polynomials of
+// `limbs` limbs at A: one launch_ntt (then, separately, launch_intt) call per
+// polynomial, averaged over `iters` passes after one warm-up pass.  With
+// `restore` non-null every call is preceded by the reference's device-to-
+// device copy of that polynomial from `restore` (v04:984).  Returns the
+// CUDA error code; ms_* receive milliseconds per pass over all polynomials.
+int ref_gpu_time16(uint32_t* A, const uint32_t* restore, const uint32_t* tw,
+                   const uint32_t* itw, const uint32_t* moduli, const uint32_t* q_inv,
+                   const uint32_t* r2, const uint32_t* dinv, size_t limbs, int polys,
+                   int iters, float* ms_ntt, float* ms_intt) {
+    const size_t words = limbs << 16;
+    auto pass = [&](bool fwd) {
+        for (int p = 0; p < polys; ++p) {
+            uint32_t* a = A + (size_t)p * words;
+            if (restore)
+                cudaMemcpy(a, restore + (size_t)p * words, words * 4, cudaMemcpyDeviceToDevice);
+            if (fwd) launch_ntt<DefaultNTTLaunchConfig<16>>(a, tw, moduli, q_inv, r2, limbs);
+            else launch_intt<DefaultNTTLaunchConfig<16>>(a, itw, moduli, q_inv, dinv, limbs);
+        }
+    };
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float* out[2] = {ms_ntt, ms_intt};
+    for (int d = 0; d < 2; ++d) {
+        pass(d == 0);
+        cudaEventRecord(e0);
+        for (int i = 0; i < iters; ++i) pass(d == 0);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        *out[d] = ms / (float)iters;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return (int)cudaDeviceSynchronize();
+}
+
 }  // extern "C"

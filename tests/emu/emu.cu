@@ -49,17 +49,21 @@ struct EmuCluster {
     std::string err;
 };
 
+// Global words of polynomial p of a job are addressed as (p << kPolyShift) +
+// word index (the pass code only adds offsets below 2^kPolyShift).
+constexpr uint32_t kPolyShift = 24;
+
 template <bool Staged>
 struct EmuCtx {
     static constexpr bool kStaged = Staged;
     EmuCluster* cl;
-    uint32_t* g;
+    uint32_t** gp;  // the job's polynomials (limb words each)
     uint32_t glen;
     const TwPair* twp;
     uint32_t twlen;
     uint32_t q, q2, rank;
     uint32_t tid = 0, seq = 0;
-    std::vector<uint32_t>* gwrites;
+    std::vector<uint32_t>* gwrites;  // per polynomial
 
     void fail(const char* what, uint64_t v) {
         if (cl->err.empty()) {
@@ -69,50 +73,50 @@ struct EmuCtx {
             cl->err = b;
         }
     }
-    // global: base and offsets are word indices into the limb
-    uint32_t g_base(uint32_t o) { return o; }
+    // global: base and offsets are word indices into the limb of polynomial p
+    uint32_t g_base(int p, uint32_t o) { return ((uint32_t)p << kPolyShift) + o; }
     uint32_t g_ld(uint32_t b, uint32_t c) {
-        const uint32_t o = b + c;
+        const uint32_t p = (b + c) >> kPolyShift, o = (b + c) & ((1u << kPolyShift) - 1u);
         if (o >= glen) {
             fail("g_ld out of range", o);
             return 0;
         }
-        return g[o];
+        return gp[p][o];
     }
     void g_ld4(uint32_t b, uint32_t c, uint32_t& x, uint32_t& y, uint32_t& z, uint32_t& w) {
-        const uint32_t o = b + c;
+        const uint32_t p = (b + c) >> kPolyShift, o = (b + c) & ((1u << kPolyShift) - 1u);
         if (o % 4 || o + 3 >= glen) {
             fail("g_ld4 out of range or misaligned", o);
             x = y = z = w = 0;
             return;
         }
-        x = g[o];
-        y = g[o + 1];
-        z = g[o + 2];
-        w = g[o + 3];
+        x = gp[p][o];
+        y = gp[p][o + 1];
+        z = gp[p][o + 2];
+        w = gp[p][o + 3];
     }
     // transform output (in place)
-    uint32_t o_base(uint32_t o) { return o; }
+    uint32_t o_base(int p, uint32_t o) { return ((uint32_t)p << kPolyShift) + o; }
     void o_st(uint32_t b, uint32_t c, uint32_t v) {
-        const uint32_t o = b + c;
+        const uint32_t p = (b + c) >> kPolyShift, o = (b + c) & ((1u << kPolyShift) - 1u);
         if (o >= glen) {
             fail("o_st out of range", o);
             return;
         }
-        g[o] = v;
-        (*gwrites)[o]++;
+        gp[p][o] = v;
+        gwrites[p][o]++;
     }
     void o_st4(uint32_t b, uint32_t c, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
-        const uint32_t o = b + c;
+        const uint32_t p = (b + c) >> kPolyShift, o = (b + c) & ((1u << kPolyShift) - 1u);
         if (o % 4 || o + 3 >= glen) {
             fail("o_st4 out of range or misaligned", o);
             return;
         }
-        g[o] = x;
-        g[o + 1] = y;
-        g[o + 2] = z;
-        g[o + 3] = w;
-        for (int i = 0; i < 4; ++i) (*gwrites)[o + i]++;
+        gp[p][o] = x;
+        gp[p][o + 1] = y;
+        gp[p][o + 2] = z;
+        gp[p][o + 3] = w;
+        for (int i = 0; i < 4; ++i) gwrites[p][o + i]++;
     }
     // stage buffer
     uint32_t st_base(uint32_t w) { return w; }
@@ -252,7 +256,18 @@ int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::strin
     cl.shadow.assign(G::C, std::vector<uint32_t>(G::SMEM_WORDS, 0));
     cl.rwrites.assign(G::C, std::vector<uint32_t>(G::SMEM_WORDS, 0));
     cl.writer.assign(G::C, std::vector<uint32_t>(G::SMEM_WORDS, 0xFFFFFFFFu));
-    std::vector<uint32_t> gw(1u << G::LOGN, 0);
+    // the job's polynomials: poly 0 is the limb itself, poly p > 0 a
+    // permutation of its words (inputs stay in range), checked at the end
+    // against the one-polynomial geometry on the same input
+    constexpr int NP = G::NP;
+    constexpr uint32_t N = 1u << G::LOGN;
+    std::vector<std::vector<uint32_t>> pw(NP, std::vector<uint32_t>(N));
+    std::vector<uint32_t*> gp(NP);
+    for (int p = 0; p < NP; ++p) {
+        for (uint32_t i = 0; i < N; ++i) pw[p][i] = p == 0 ? limb[i] : limb[(N - 1 - i + p) % N];
+        gp[p] = pw[p].data();
+    }
+    std::vector<std::vector<uint32_t>> gw(NP, std::vector<uint32_t>(N, 0));
     // the kernel's bulk copies of the input slab into each CTA's stage buffer
     cl.stage.assign(G::C, std::vector<uint32_t>(G::STAGE_WORDS, 0xDEADBEEFu));
     for (uint32_t r = 0; r < (uint32_t)G::C; ++r) {
@@ -276,8 +291,8 @@ int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::strin
             }
     }
     auto mk = [&](uint32_t rank) {
-        Ctx c{&cl, limb, 1u << G::LOGN, tw, 1u << G::LOGN, q, 2 * q, rank};
-        c.gwrites = &gw;
+        Ctx c{&cl, gp.data(), 1u << G::LOGN, tw, 1u << G::LOGN, q, 2 * q, rank};
+        c.gwrites = gw.data();
         return c;
     };
     using F = Forward<G, Arith, Ctx>;
@@ -306,11 +321,12 @@ int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::strin
     // every non-pad work-buffer word written exactly once by the last step
     auto check_cover = [&](const char* what) {
         for (int r = 0; r < G::C; ++r)
-            for (uint32_t lam = 0; lam < G::M; ++lam)
-                if (cl.writes[r][G::XW::phys(lam)] != 1) {
-                    if (err.empty()) err = std::string(what) + ": word not written exactly once";
-                    return;
-                }
+            for (int p = 0; p < NP; ++p)
+                for (uint32_t lam = 0; lam < G::M; ++lam)
+                    if (cl.writes[r][p * G::SLAB_WORDS + G::XW::phys(lam)] != 1) {
+                        if (err.empty()) err = std::string(what) + ": word not written exactly once";
+                        return;
+                    }
     };
     if (Fwd) {
         step([](Ctx& c, uint32_t t) { F::pass1a(c, t); }, false);
@@ -341,10 +357,27 @@ int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::strin
         }
         step([](Ctx& c, uint32_t t) { I::pass1a(c, t); }, G::K1B > 0 && G::WARP1);
     }
-    for (uint32_t i = 0; i < (1u << G::LOGN); ++i)
-        if (gw[i] != 1 && err.empty()) err = "global word not written exactly once";
+    for (int p = 0; p < NP; ++p)
+        for (uint32_t i = 0; i < N; ++i)
+            if (gw[p][i] != 1 && err.empty()) err = "global word not written exactly once";
     if (!cl.err.empty() && err.empty()) err = cl.err;
-    return err.empty() ? 0 : 1;
+    if (!err.empty()) return 1;
+    if constexpr (NP > 1) {
+        // every polynomial of the job equals its own one-polynomial transform
+        using G1 = Geometry<G::LOGN, G::CLOG, G::R1, G::EB, G::K1A, G::K2A, 1>;
+        for (int p = 1; p < NP; ++p) {
+            std::vector<uint32_t> one(N);
+            for (uint32_t i = 0; i < N; ++i) one[i] = limb[(N - 1 - i + p) % N];
+            Stats st1;
+            if (run_limb<G1, Arith, Fwd, false>(one.data(), tw, q, st1, err)) return 1;
+            if (one != pw[p]) {
+                err = "polynomial " + std::to_string(p) + " of a job differs from its own transform";
+                return 1;
+            }
+        }
+    }
+    std::copy(pw[0].begin(), pw[0].end(), limb);
+    return 0;
 }
 
 template <class G, bool Staged>
@@ -373,19 +406,21 @@ int run_cfg(int fwd, uint32_t* data, const uint32_t* tw_pairs, const uint32_t* q
 using RunFn = int (*)(int, uint32_t*, const uint32_t*, const uint32_t*, int, double*,
                       std::string&);
 struct Entry {
-    int v[6];
+    int v[7];
     int threads;
     unsigned smem;
     RunFn staged, direct;
 };
 
-#define EMU_G(N, CL, R1, EB, K1A, K2A) Geometry<N, CL, R1, EB, K1A, K2A>
-#define EMU_ENTRY(N, CL, R1, EB, K1A, K2A)                                                 \
-    {{N, CL, R1, EB, K1A, K2A},                                                            \
-     EMU_G(N, CL, R1, EB, K1A, K2A)::THREADS,                                              \
-     EMU_G(N, CL, R1, EB, K1A, K2A)::SMEM_BYTES,                                           \
-     &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A), true>,                                       \
-     &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A), false>},
+// NP > 1 has no staged form: its staged entry runs the direct passes, as
+// the library's does.
+#define EMU_G(N, CL, R1, EB, K1A, K2A, NP) Geometry<N, CL, R1, EB, K1A, K2A, NP>
+#define EMU_ENTRY(N, CL, R1, EB, K1A, K2A, NP)                                             \
+    {{N, CL, R1, EB, K1A, K2A, NP},                                                        \
+     EMU_G(N, CL, R1, EB, K1A, K2A, NP)::THREADS,                                          \
+     EMU_G(N, CL, R1, EB, K1A, K2A, NP)::SMEM_BYTES,                                       \
+     &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A, NP), (NP) == 1>,                              \
+     &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A, NP), false>},
 const Entry kEntries[] = {NTTB_CFG_ALL(EMU_ENTRY)};
 std::string g_err;
 
@@ -393,10 +428,11 @@ std::string g_err;
 
 extern "C" {
 int emu_num_configs() { return (int)(sizeof(kEntries) / sizeof(kEntries[0])); }
-void emu_config(int i, int* out8) {
-    for (int k = 0; k < 6; ++k) out8[k] = kEntries[i].v[k];
-    out8[6] = kEntries[i].threads;
-    out8[7] = (int)kEntries[i].smem;
+// out9: N, CL, R1, EB, K1A, K2A, NP, threads, shared-memory bytes
+void emu_config(int i, int* out9) {
+    for (int k = 0; k < 7; ++k) out9[k] = kEntries[i].v[k];
+    out9[7] = kEntries[i].threads;
+    out9[8] = (int)kEntries[i].smem;
 }
 // data: limbs * N words in place; tw_pairs: limbs * N (w, w') pairs.
 // mode bit 0: forward (else inverse); bit 1: direct input (else staged).

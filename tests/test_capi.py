@@ -99,6 +99,8 @@ def test_config_catalogue_covers_every_size():
         assert c.threads in (32, 64, 128, 256, 512, 1024)
         assert c.smem_bytes <= 227 * 1024
         assert c.cluster_ctas in (1, 2, 4, 8, 16)
+        assert c.polys_per_job in (1, 2)
+    assert any(c.polys_per_job == 2 for c in cfgs)
 
 
 def test_plan_without_device_fails_cleanly():

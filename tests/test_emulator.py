@@ -37,16 +37,18 @@ def configs():
     src = open(os.path.join(os.path.dirname(__file__), "..", "ntt_b200", "csrc", "configs.h")).read()
     body = src.split("#define NTTB_CFG_ALL")[0]
     return [tuple(int(v) for v in m) for m in
-            re.findall(r"X\((\d+), (\d+), (\d+), (\d+), (\d+), (\d+)\)", body)]
+            re.findall(r"X\((\d+), (\d+), (\d+), (\d+), (\d+), (\d+), (\d+)\)", body)]
 
 
 @pytest.mark.parametrize("idx,cfg", list(enumerate(configs())), ids=lambda v: str(v))
 @pytest.mark.parametrize("bits", [30, 31])
 @pytest.mark.parametrize("direct", [0, 2], ids=["staged", "direct"])
 def test_config_matches_oracle(emu, idx, cfg, bits, direct):
-    c = (ctypes.c_int * 8)()
+    if cfg[6] > 1 and direct == 0:
+        pytest.skip("several polynomials per job: no staged form (its staged entry is the direct run)")
+    c = (ctypes.c_int * 9)()
     emu.emu_config(idx, c)
-    assert tuple(c)[:6] == cfg
+    assert tuple(c)[:7] == cfg
     logN = cfg[0]
     start = int(2 ** 29.5) if bits == 30 else int(2 ** 30.5)
     mods = O.ascending_primes(logN, 2, start)

@@ -1,0 +1,125 @@
+"""Plan-level negacyclic product (ntt_multiply_many: NTT(b), NTT(a) with the
+pointwise Montgomery product folded into its store, INTT(b)) against the
+unfused plain calls (forward, forward, ntt_pointwise_mul, inverse) and the
+schoolbook product mod q.  Needs a B200.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def nb(torch_cuda):
+    import ntt_b200
+    return ntt_b200
+
+
+@pytest.fixture(scope="module")
+def mixes(nb):
+    from ntt_b200 import mixes
+    return mixes
+
+
+def host(t):
+    return t.cpu().numpy().view(np.uint32)
+
+
+def pair_inputs(torch, mixes, nb, logN, mods, pairs, seed):
+    job = mixes.MixJob(nb.OP_MULTIPLY, logN, mods)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    a = torch.stack([mixes.uniform_device(torch, job, g) for _ in range(pairs)])
+    b = torch.stack([mixes.uniform_device(torch, job, g) for _ in range(pairs)])
+    return a, b
+
+
+def unfused(p, a, b, pairs):
+    ta, tb = a.clone(), b.clone()
+    p.forward_many(ta, pairs)
+    p.forward_many(tb, pairs)
+    p.pointwise_mul(tb, ta, tb, pairs)
+    p.inverse_many(tb, pairs)
+    return tb
+
+
+@pytest.mark.parametrize("logN,bits", [(10, 30), (12, 31), (13, 30), (14, 31), (15, 30),
+                                       (16, 31), (17, 30)])
+def test_multiply_many_matches_unfused(torch_cuda, nb, mixes, logN, bits):
+    torch = torch_cuda
+    pairs, limbs = 3, 5
+    mods = list(mixes.prime_pool(logN, bits, limbs))
+    a, b = pair_inputs(torch, mixes, nb, logN, mods, pairs, 70 + logN)
+    a_h = host(a).copy()
+    p = nb.Plan(logN, mods)
+    expect = unfused(p, a, b, pairs)
+    p.multiply_many(a, b, pairs)
+    torch.cuda.synchronize()
+    assert torch.equal(b, expect)
+    assert np.array_equal(host(a), a_h)  # the factor a is read only
+    assert p.check() == 0
+    p.close()
+
+
+def test_multiply_many_every_logn16_config(torch_cuda, nb, mixes):
+    """Every compiled logN-16 configuration (one and two polynomials per job),
+    an odd number of pairs (the last two-polynomial job repeats a pair)."""
+    torch = torch_cuda
+    pairs, limbs = 5, 3
+    mods = list(mixes.prime_pool(16, 30, limbs))
+    a, b = pair_inputs(torch, mixes, nb, 16, mods, pairs, 5)
+    ref = nb.Plan(16, mods)
+    expect = unfused(ref, a, b, pairs)
+    for idx, c in enumerate(nb.kernel_configs()):
+        if c.logN != 16:
+            continue
+        p = nb.Plan(16, mods)
+        p.force_config(idx, idx)
+        x = b.clone()
+        p.multiply_many(a, x, pairs)
+        torch.cuda.synchronize()
+        assert torch.equal(x, expect), f"config {idx}"
+        p.close()
+    ref.close()
+
+
+def test_multiply_many_schoolbook_sample(torch_cuda, nb, mixes):
+    """The fused multiply configuration's shape (2^16, 24 limbs of 30-bit
+    primes): 64 sampled (pair, limb, coefficient) triples against the O(N)
+    schoolbook negacyclic coefficient mod q."""
+    torch = torch_cuda
+    logN, pairs, limbs = 16, 2, 24
+    mods = list(mixes.prime_pool(logN, 30, limbs))
+    a, b = pair_inputs(torch, mixes, nb, logN, mods, pairs, 9)
+    a_h, b_h = host(a).copy(), host(b).copy()
+    p = nb.Plan(logN, mods)
+    p.multiply_many(a, b, pairs)
+    torch.cuda.synchronize()
+    c = host(b)
+    rng = np.random.default_rng(16)
+    for _ in range(64):
+        i, l, k = int(rng.integers(pairs)), int(rng.integers(limbs)), int(rng.integers(1 << logN))
+        assert int(c[i, l, k]) == O.negacyclic_coeff(a_h[i, l], b_h[i, l], logN, mods[l][0], k)
+    p.close()
+
+
+def test_multiply_many_errors(torch_cuda, nb, mixes):
+    torch = torch_cuda
+    mods = list(mixes.prime_pool(12, 30, 2))
+    p = nb.Plan(12, mods)
+    x = torch.zeros(4, 2 << 12, dtype=torch.int32, device="cuda")
+    with pytest.raises(nb.NttError) as e:  # b overlaps a
+        p.multiply_many(x[0], x[0], 1)
+    assert e.value.name == "NTT_ERR_INVALID_ARGUMENT"
+    with pytest.raises(nb.NttError) as e:
+        p.multiply_many(x[0].data_ptr() + 4, x[2], 1)
+    assert e.value.name == "NTT_ERR_MISALIGNED"
+    p.close()
+    small = nb.Plan(8, list(mixes.prime_pool(8, 30, 1)))
+    y = torch.zeros(2, 1 << 8, dtype=torch.int32, device="cuda")
+    with pytest.raises(nb.NttError) as e:
+        small.multiply_many(y[0], y[1], 1)
+    assert e.value.name == "NTT_ERR_UNSUPPORTED"
+    small.close()
