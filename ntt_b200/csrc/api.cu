@@ -82,6 +82,30 @@ const FusedConfig* default_config(int logN, bool fwd) {
     return nullptr;
 }
 
+// Configuration for launches of a single polynomial (one wave of clusters or
+// less, so latency-bound): the pick measured fastest for single-polynomial
+// calls on B200, else the default for (logN, direction) when it carries one
+// polynomial per job, else the first such configuration.
+const FusedConfig* default_single_config(int logN, bool fwd) {
+    struct Pick {
+        int logN, clog, r1, eb, k1a, k2a;
+        bool fwd;
+    };
+    static const Pick picks[] = {{16, 3, 8, 4, 4, 4, true}, {16, 3, 8, 4, 4, 4, false}};
+    const FusedConfig* c = fused_configs();
+    for (const Pick& p : picks)
+        if (p.logN == logN && p.fwd == fwd)
+            for (int i = 0; i < fused_config_count(); ++i)
+                if (c[i].logN == p.logN && c[i].clog == p.clog && c[i].r1 == p.r1 &&
+                    c[i].eb == p.eb && c[i].k1a == p.k1a && c[i].k2a == p.k2a && c[i].np == 1)
+                    return &c[i];
+    const FusedConfig* d = default_config(logN, fwd);
+    if (!d || d->np == 1) return d;
+    for (int i = 0; i < fused_config_count(); ++i)
+        if (c[i].logN == logN && c[i].np == 1) return &c[i];
+    return d;
+}
+
 const FusedConfig* config_by_r1(int logN, int r1) {
     const FusedConfig* c = fused_configs();
     for (int i = 0; i < fused_config_count(); ++i)
@@ -246,6 +270,10 @@ struct ntt_plan {
     size_t bytes = 0;
     const FusedConfig* cfg_fwd = nullptr;  // nullptr: small kernel
     const FusedConfig* cfg_inv = nullptr;
+    // launches with fewer polynomials than cfg_*'s polynomials per job (a
+    // single-polynomial call of a two-polynomial configuration) use these
+    const FusedConfig* cfg_fwd1 = nullptr;
+    const FusedConfig* cfg_inv1 = nullptr;
     TransformConfig effective{};
     int tuned = 0;
     int schedule = NTT_SCHEDULE_DIRECT;
@@ -323,6 +351,9 @@ void choose_configs(ntt_plan* p, const TransformConfig* t) {
         if (auto c = config_by_r1(p->logN, t->ntt_phase1.radix_stages)) p->cfg_fwd = c;
         if (auto c = config_by_r1(p->logN, t->intt_phase2.radix_stages)) p->cfg_inv = c;
     }
+    // single-polynomial launches: an explicit phase split still applies
+    p->cfg_fwd1 = (t && p->cfg_fwd->np == 1) ? p->cfg_fwd : default_single_config(p->logN, true);
+    p->cfg_inv1 = (t && p->cfg_inv->np == 1) ? p->cfg_inv : default_single_config(p->logN, false);
 }
 
 }  // namespace nttb
@@ -505,6 +536,8 @@ ntt_status_t ntt_plan_force_config(ntt_plan_t* p, int fwd_index, int inv_index) 
         return fail(NTT_ERR_INVALID_ARGUMENT, "configuration index does not match logN %d", p->logN);
     p->cfg_fwd = f;
     p->cfg_inv = i;
+    p->cfg_fwd1 = f;  // a pinned configuration runs every launch
+    p->cfg_inv1 = i;
     effective_triples(p->cfg_fwd, p->logN, &p->effective);
     TransformConfig ti;
     effective_triples(p->cfg_inv, p->logN, &ti);
@@ -590,7 +623,9 @@ static ntt_status_t plan_run(const ntt_plan_t* p, uint32_t* a, size_t polys, siz
         return fail(NTT_ERR_INVALID_ARGUMENT, "plan was created on device %d, current is %d",
                     p->device, dev);
     if (stride == 0) stride = (size_t)p->limbs << p->logN;
-    return run_transform(p->logN, fwd ? p->cfg_fwd : p->cfg_inv, fwd ? p->fwd : p->inv, p->q,
+    const FusedConfig* cfg = fwd ? p->cfg_fwd : p->cfg_inv;
+    if (cfg && (polys == 1 || polys < (size_t)cfg->np)) cfg = fwd ? p->cfg_fwd1 : p->cfg_inv1;
+    return run_transform(p->logN, cfg, fwd ? p->fwd : p->inv, p->q,
                          p->limbs, a, polys, stride, fwd, (cudaStream_t)s, p->status,
                          p->schedule, p->lazy2);
 }
@@ -654,14 +689,18 @@ ntt_status_t ntt_multiply_many(const ntt_plan_t* p, const uint32_t* a, uint32_t*
         return fail(NTT_ERR_INVALID_ARGUMENT, "plan was created on device %d, current is %d",
                     p->device, dev);
     const cudaStream_t cs = (cudaStream_t)s;
+    const FusedConfig* cf =
+        (polys == 1 || polys < (size_t)p->cfg_fwd->np) ? p->cfg_fwd1 : p->cfg_fwd;
+    const FusedConfig* ci =
+        (polys == 1 || polys < (size_t)p->cfg_inv->np) ? p->cfg_inv1 : p->cfg_inv;
     // b <- NTT(b); b <- NTT(a) (.) b (product fused into the forward's store); b <- INTT(b)
-    if (ntt_status_t st = run_transform(p->logN, p->cfg_fwd, p->fwd, p->q, p->limbs, b, polys,
-                                        stride, true, cs, p->status, p->schedule, p->lazy2))
+    if (ntt_status_t st = run_transform(p->logN, cf, p->fwd, p->q, p->limbs, b, polys, stride,
+                                        true, cs, p->status, p->schedule, p->lazy2))
         return st;
-    if (ntt_status_t st = run_transform(p->logN, p->cfg_fwd, p->fwd, p->q, p->limbs, b, polys,
-                                        stride, true, cs, p->status, p->schedule, p->lazy2, a))
+    if (ntt_status_t st = run_transform(p->logN, cf, p->fwd, p->q, p->limbs, b, polys, stride,
+                                        true, cs, p->status, p->schedule, p->lazy2, a))
         return st;
-    return run_transform(p->logN, p->cfg_inv, p->inv, p->q, p->limbs, b, polys, stride, false, cs,
+    return run_transform(p->logN, ci, p->inv, p->q, p->limbs, b, polys, stride, false, cs,
                          p->status, p->schedule, p->lazy2);
 }
 
@@ -740,8 +779,8 @@ ntt_status_t shim_run(uint32_t* A, const uint32_t* tw, const uint32_t* moduli, c
         // column stages: NTT phase 1 / INTT phase 2 (the second triple)
         const PhaseConfig* col = inverse ? ph2 : ph1;
         cfg = col ? config_by_r1(logN, col->radix_stages) : nullptr;
-        if (!cfg) cfg = tuned_config(logN, (int)limbs, !inverse);
-        if (!cfg) cfg = default_config(logN, !inverse);
+        // one polynomial per call: the single-polynomial choice
+        if (!cfg) cfg = default_single_config(logN, !inverse);
     }
     return run_transform(logN, cfg, table, moduli, (int)limbs, A, 1, limbs << logN, !inverse, 0,
                          nullptr, NTT_SCHEDULE_DIRECT, lazy2);

@@ -323,7 +323,11 @@ struct Maps {
 // Fold: the limb's stage 0 (one twiddle, index 1) with the factor in entry 0.
 // v[p][r]: register r of polynomial p; every twiddle loaded once serves the
 // same butterfly of all NP polynomials of the job.
-template <class L, class Arith, bool Fwd, int k, bool Fold, int NP, class Ctx>
+// Perm != 0: the stage's twiddle block (starting at index H) is stored
+// interleaved by Perm (tw_slot, arith.cuh): entry H + j at slot
+// H + (j % Perm) * S16 + j / Perm.
+template <class L, class Arith, bool Fwd, int k, bool Fold, int NP, int Perm = 0,
+          uint32_t H = 0, uint32_t S16 = 0, class Ctx>
 NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
     constexpr int p = Fwd ? (L::PLO + L::KB - 1 - k) : (L::PLO + k);
     constexpr int gbits = Fwd ? k : (L::KB - 1 - k);
@@ -349,16 +353,41 @@ NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
         ct_for<(1 << XHB)>([&](auto XH) {
             constexpr int xh = decltype(XH)::value;
             constexpr uint32_t xoff = L::off(xh << XLB) >> (p + 1);
-            auto tb = ctx.tw_base(tbase + xoff);
-            // twiddles of this stage for this xh: 2^gbits consecutive pairs
+            // twiddles of this stage for this xh: 2^gbits consecutive entries
             TwPair w[1 << gbits];
-            if constexpr (gbits >= 1) {
-                ct_for<(1 << (gbits - 1))>([&](auto G2) {
-                    constexpr int g2 = decltype(G2)::value;
-                    ctx.tw_ld2(tb, 2 * g2, w[2 * g2], w[2 * g2 + 1]);
-                });
+            if constexpr (Perm == 0) {
+                auto tb = ctx.tw_base(tbase + xoff);
+                if constexpr (gbits >= 1) {
+                    ct_for<(1 << (gbits - 1))>([&](auto G2) {
+                        constexpr int g2 = decltype(G2)::value;
+                        ctx.tw_ld2(tb, 2 * g2, w[2 * g2], w[2 * g2 + 1]);
+                    });
+                } else {
+                    w[0] = ctx.tw_ld(tb, 0);
+                }
             } else {
-                w[0] = ctx.tw_ld(tb, 0);
+                constexpr int lp = Perm == 8 ? 3 : 2;
+                // the thread's part of the entry index, j0 = tbase - H, is a
+                // multiple of Perm when the lambda bits p+1 .. p+lp are
+                // register bits (zero in the thread's base): then the slot of
+                // entry j0 + c is (H + j0 / Perm) + a compile-time offset
+                constexpr bool kAligned =
+                    ((L::kRegMask >> (p + 1)) & (uint32_t)(Perm - 1)) == (uint32_t)(Perm - 1);
+                const uint32_t j0 = tbase - H;
+                if constexpr (kAligned) {
+                    auto tb = ctx.tw_base(H + (j0 >> lp));
+                    ct_for<(1 << gbits)>([&](auto Gc) {
+                        constexpr uint32_t c = xoff + decltype(Gc)::value;
+                        w[decltype(Gc)::value] =
+                            ctx.tw_ld(tb, (c & (uint32_t)(Perm - 1)) * S16 + (c >> lp));
+                    });
+                } else {
+                    ct_for<(1 << gbits)>([&](auto Gc) {
+                        const uint32_t j = j0 + xoff + decltype(Gc)::value;
+                        w[decltype(Gc)::value] =
+                            ctx.tw_at(H + (j & (uint32_t)(Perm - 1)) * S16 + (j >> lp));
+                    });
+                }
             }
             ct_for<(1 << gbits)>([&](auto Gc) {
                 constexpr int g = decltype(Gc)::value;
@@ -398,7 +427,13 @@ NTT_HD void run_stages(Ctx& ctx, uint32_t (&v)[G::NP][L::E], uint32_t d) {
         constexpr bool s0 = HasStage0 && (Fwd ? (k == 0) : (k == L::KB - 1));
         const uint32_t tb =
             (Phase2 ? Mp::tw_base_p2(p, ctx.rank) : Mp::tw_base_p1(p)) + (d >> (p + 1));
-        stage<L, Arith, Fwd, k, s0, G::NP>(ctx, v, tb);
+        // phase-2 bit 0 / 1 is the limb's stage logN-1 / logN-2, whose
+        // twiddles are stored interleaved (tw_slot)
+        constexpr bool kPermLayout = Phase2 && G::LOGN >= kTwPermMinLogN && p <= 1;
+        constexpr int perm = kPermLayout ? (p == 0 ? 8 : 4) : 0;
+        constexpr uint32_t h = kPermLayout ? (1u << (G::LOGN - 1 - p)) : 0u;
+        constexpr uint32_t s16 = kPermLayout ? (1u << (G::LOGN - 4)) : 0u;
+        stage<L, Arith, Fwd, k, s0, G::NP, perm, h, s16>(ctx, v, tb);
         if constexpr (ArriveAfterFirst && k == 0) ctx.after_local_reads();
     });
 }

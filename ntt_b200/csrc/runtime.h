@@ -15,6 +15,8 @@ ntt_status_t cuda_fail(cudaError_t e, const char* what);
 
 // Untuned default for (logN, direction); config_by_r1 matches a phase split.
 const FusedConfig* default_config(int logN, bool fwd = true);
+// ... for launches of a single polynomial (one polynomial per job).
+const FusedConfig* default_single_config(int logN, bool fwd);
 const FusedConfig* config_by_r1(int logN, int r1);
 const FusedConfig* config_by_index(int idx);
 // Autotuned choice for (logN, limbs, direction) on the current device, or

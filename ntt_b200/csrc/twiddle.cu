@@ -13,6 +13,8 @@
 //                                         v04:567-580, folded into the last
 //                                         stage: N^-1 and from_mont)
 //            entry 1: psi^-bitrev(1) * c
+// Entry i is stored at slot tw_slot(i, logN) (arith.cuh): the last two stages'
+// blocks are interleaved for coalesced loads.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "arith.cuh"
@@ -53,7 +55,8 @@ __global__ void twiddle_gen_kernel(TwPair* out, const TwGenLimb* limbs, int logN
         }
         w = dev_redc(acc, L.q, L.nqinv);  // leave the Montgomery domain
     }
-    out[(size_t)blockIdx.y * N + i] = TwPair{w, (uint32_t)(((uint64_t)w << 32) / L.q)};
+    out[(size_t)blockIdx.y * N + tw_slot(i, logN)] =
+        TwPair{w, (uint32_t)(((uint64_t)w << 32) / L.q)};
 }
 
 // Import the reference's Montgomery-form tables (tw_mont[i] = to_mont(w_i)).
@@ -79,7 +82,7 @@ __global__ void twiddle_import_kernel(TwPair* out, const uint32_t* tw_mont,
         else if (i == 1) w = (uint32_t)(((uint64_t)dev_redc(t[1], q, qi) * c) % q);
         else w = dev_redc(t[i], q, qi);
     }
-    out[(size_t)l * N + i] = TwPair{w, (uint32_t)(((uint64_t)w << 32) / q)};
+    out[(size_t)l * N + tw_slot(i, logN)] = TwPair{w, (uint32_t)(((uint64_t)w << 32) / q)};
 }
 
 cudaError_t launch_twiddle_gen(TwPair* out, const TwGenLimb* limbs_dev, int limbs, int logN,

@@ -6,10 +6,27 @@ Shoup companion floor(w * 2^32 / q), with entries 0 and 1 replaced by the
 constants folded into limb stage 0:
   forward  [0] = R mod q, [1] = psi^bitrev(1) * R   (R = 2^32: Montgomery form)
   inverse  [0] = c = N^-1 * R^-1, [1] = psi^-bitrev(1) * c
+For logN >= 10 entry i is stored at slot tw_slot(i) below: the blocks of the
+last two stages are interleaved by 8 and 4 (entry N/2 + j at slot
+N/2 + (j % 8) * N/16 + j // 8; entry N/4 + j at N/4 + (j % 4) * N/16 + j // 4).
 This module rebuilds that layout from the oracle so the CPU emulator and the
 GPU table check have an independent expected value.
 """
 import numpy as np
+
+PERM_MIN_LOGN = 10
+
+
+def tw_slot(i: int, logN: int) -> int:
+    if logN < PERM_MIN_LOGN:
+        return i
+    N = 1 << logN
+    h, qt, s16 = N // 2, N // 4, N // 16
+    if i >= h:
+        return h + ((i - h) % 8) * s16 + (i - h) // 8
+    if i >= qt:
+        return qt + ((i - qt) % 4) * s16 + (i - qt) // 4
+    return i
 
 
 def _pair(w: int, q: int):
@@ -36,4 +53,8 @@ def device_tables(T):
         fwd[l, 1] = _pair(int(T.psi_tab[l, 1]) * R, q)
         inv[l, 0] = _pair(c, q)
         inv[l, 1] = _pair(int(T.inv_tab[l, 1]) * c, q)
-    return fwd, inv
+    slots = np.array([tw_slot(i, T.logN) for i in range(N)])
+    pf, pi = np.empty_like(fwd), np.empty_like(inv)
+    pf[:, slots] = fwd
+    pi[:, slots] = inv
+    return pf, pi
