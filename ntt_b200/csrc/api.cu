@@ -66,7 +66,7 @@ const FusedConfig* default_config(int logN, bool fwd) {
         int logN, clog, r1, eb, k1a, k2a, np;
         bool fwd;
     };
-    static const Pick picks[] = {{16, 3, 8, 5, 3, 4, 1, true}, {16, 4, 8, 4, 4, 4, 2, false},
+    static const Pick picks[] = {{16, 3, 8, 5, 3, 4, 1, true}, {16, 3, 7, 5, 3, 5, 1, false},
                                  {17, 4, 8, 5, 3, 5, 1, true}, {17, 4, 8, 5, 3, 5, 1, false},
                                  {15, 1, 10, 5, 5, 5, 1, false}};
     const FusedConfig* c = fused_configs();

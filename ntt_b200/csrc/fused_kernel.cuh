@@ -278,6 +278,8 @@ __device__ __forceinline__ void fused_forward_body(Ctx& ctx, Pre&& prefetch) {
     if constexpr (G::K2B > 0) {
         pass_sync<G::WARP2>();
         F::pass2b(ctx, tid);
+        pass_sync<G::WARP2>();  // the warp's chunk is the words it wrote
+        F::pass2c(ctx, tid);
     }
 }
 
@@ -285,6 +287,10 @@ template <class G, class Arith, class Ctx, class Pre>
 __device__ __forceinline__ void fused_inverse_body(Ctx& ctx, Pre&& prefetch) {
     using I = Inverse<G, Arith, Ctx>;
     const uint32_t tid = threadIdx.x;
+    if constexpr (I::kChunkIn) {
+        I::pass2c(ctx, tid);
+        pass_sync<G::WARP2>();  // the warp's chunk holds its pass-2b words
+    }
     if constexpr (G::K2B > 0) {
         I::pass2b(ctx, tid);
         pass_sync<G::WARP2>();

@@ -620,6 +620,59 @@ NTT_HD void scatter_regs(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t dd, uint32_
     });
 }
 
+// The contiguous phase-2 slab [rank*M, (rank+1)*M) of the limb moves between
+// global memory and the work buffer in warp chunks: warp w owns the
+// M / warps consecutive words from w * M / warps (exactly its elements in the
+// phase-2 register passes when they are warp-owned), and lane l moves words
+// l, l + 32, l + 64, ... of the chunk, so every warp instruction touches one
+// 128-byte line.  A register pass's own accesses would put each lane on its
+// own line (a thread holds runs of consecutive words), which costs the L1
+// pipe 32 wavefronts per instruction instead of one to four.
+template <class G>
+struct SlabChunk {
+    static constexpr uint32_t WARPS = G::THREADS / 32u;
+    static constexpr uint32_t WORDS = G::M / WARPS;
+    static_assert(WORDS % 32u == 0, "warp chunks of whole lines");
+    // lambda of lane 0 of this warp's chunk plus the lane (bit-disjoint from
+    // the per-step offsets 32 * i, so phys() splits into base + immediate)
+    NTT_HD static uint32_t base(uint32_t tid) { return (tid >> 5) * WORDS + (tid & 31u); }
+};
+
+// Work buffer -> global: the slab's canonical words, stored through the
+// context's o_* interface (plain store, or the product epilogue).
+template <class G, class X, class Ctx>
+NTT_HD void slab_out(Ctx& ctx, uint32_t tid) {
+    const uint32_t b = SlabChunk<G>::base(tid);
+    auto sb = ctx.s_base(X::phys(b));
+    ct_for<G::NP>([&](auto Pp) {
+        constexpr int pp = decltype(Pp)::value;
+        auto gb = ctx.o_base(pp, b + ctx.rank * G::M);
+        ct_for<SlabChunk<G>::WORDS / 32u>([&](auto I) {
+            constexpr uint32_t o = 32u * decltype(I)::value;
+            ctx.o_st(gb, o, ctx.s_ld(sb, pp * G::SLAB_WORDS + X::phys(o)));
+        });
+    });
+}
+
+// Global -> work buffer: the inverse's input slab.
+template <class G, class X, class Ctx>
+NTT_HD void slab_in(Ctx& ctx, uint32_t tid) {
+    const uint32_t b = SlabChunk<G>::base(tid);
+    auto sb = ctx.s_base(X::phys(b));
+    ct_for<G::NP>([&](auto Pp) {
+        constexpr int pp = decltype(Pp)::value;
+        auto gb = ctx.g_base(pp, b + ctx.rank * G::M);
+        uint32_t w[SlabChunk<G>::WORDS / 32u];
+        ct_for<SlabChunk<G>::WORDS / 32u>([&](auto I) {
+            w[decltype(I)::value] = ctx.g_ld(gb, 32u * decltype(I)::value);
+        });
+        ct_for<SlabChunk<G>::WORDS / 32u>([&](auto I) {
+            constexpr uint32_t o = 32u * decltype(I)::value;
+            ctx.s_st(sb, pp * G::SLAB_WORDS + X::phys(o), w[decltype(I)::value]);
+        });
+    });
+}
+
 template <class G, class Arith, class Ctx>
 struct Forward {
     using Mp = Maps<G>;
@@ -671,15 +724,27 @@ struct Forward {
                                                  FwdFinal<Arith>{ctx.q, ctx.q2});
         }
     }
+    // With two phase-2 passes the last one writes its canonical words back
+    // in place and pass2c stores the slab in warp chunks (SlabChunk).
     NTT_HD static void pass2b(Ctx& ctx, uint32_t tid) {
         if constexpr (G::K2B > 0) {
             uint32_t v[G::NP][P2B::E];
             const uint32_t d = P2B::dep(tid);
             load_smem<P2B, X, G::SLAB_WORDS>(ctx, v, d);
             run_stages<G, P2B, Arith, true, true, false>(ctx, v, d);
-            store_global<P2B, (1u << 30), G2Map>(ctx, v, d + ctx.rank * G::M,
-                                                 FwdFinal<Arith>{ctx.q, ctx.q2});
+            const FwdFinal<Arith> fin{ctx.q, ctx.q2};
+            ct_for<G::NP>([&](auto Pp) {
+                ct_for<P2B::E>([&](auto R) {
+                    v[decltype(Pp)::value][decltype(R)::value] =
+                        fin(v[decltype(Pp)::value][decltype(R)::value]);
+                });
+            });
+            store_smem<P2B, X, G::SLAB_WORDS>(ctx, v, d);
         }
+    }
+    // (after a barrier over pass2b's writes)
+    NTT_HD static void pass2c(Ctx& ctx, uint32_t tid) {
+        if constexpr (G::K2B > 0) slab_out<G, X>(ctx, tid);
     }
 };
 
@@ -716,8 +781,15 @@ struct Inverse {
             store_smem<L, X, G::SLAB_WORDS>(ctx, v, d);
         }
     }
+    // With two phase-2 passes and direct input, pass2c first copies the
+    // input slab into the work buffer in warp chunks (SlabChunk); the
+    // staged schedule's first pass reads the bulk-copied stage buffer.
+    static constexpr bool kChunkIn = G::K2B > 0 && !Ctx::kStaged;
+    NTT_HD static void pass2c(Ctx& ctx, uint32_t tid) {
+        if constexpr (kChunkIn) slab_in<G, X>(ctx, tid);
+    }
     NTT_HD static void pass2b(Ctx& ctx, uint32_t tid) {
-        if constexpr (G::K2B > 0) phase2_pass<P2B, false, true>(ctx, tid);
+        if constexpr (G::K2B > 0) phase2_pass<P2B, false, !kChunkIn>(ctx, tid);
     }
     NTT_HD static void pass2a(Ctx& ctx, uint32_t tid) {
         phase2_pass<P2A, true, G::K2B == 0>(ctx, tid);
