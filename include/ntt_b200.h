@@ -146,9 +146,9 @@ NTT_API ntt_status_t ntt_plan_get_info(const ntt_plan_t* plan, ntt_plan_info_t* 
 NTT_API ntt_status_t ntt_plan_check(const ntt_plan_t* plan, uint32_t* device_status);
 /* Device pointers of the plan's tables: limbs * N (w, w') uint32 pairs, with
  * entries 0 and 1 holding the constants folded into limb stage 0, and for
- * logN >= 10 the last two stages' blocks interleaved for coalesced loads:
- * entry N/2 + j at slot N/2 + (j % 8) * (N/16) + j / 8, entry N/4 + j at slot
- * N/4 + (j % 4) * (N/16) + j / 4. */
+ * logN >= 10 the last four stages' blocks interleaved for coalesced loads:
+ * stage logN-1-p (p = 0..3) starts at H = N / 2^(p+1), and its entry H + j
+ * sits at slot H + (j % F) * (N/32) + j / F with F = 16 / 2^p. */
 NTT_API ntt_status_t ntt_plan_tables(const ntt_plan_t* plan, const uint32_t** fwd_pairs,
                              const uint32_t** inv_pairs, const uint32_t** moduli);
 

@@ -58,21 +58,29 @@ struct TwPair {
 };
 
 // Device twiddle-table layout of one limb (N = 2^logN entries).  In the last
-// two stages every thread of the transform kernels owns a run of consecutive
-// entries (8 and 4 of them for the usual 4-stage register pass), so in the
-// natural order the 32 lanes of a warp would read 32 scattered cache lines per
-// load.  Those two blocks are therefore stored interleaved, which makes the
-// lanes' loads consecutive:
-//   stage logN-1, entry N/2 + j  at slot  N/2 + (j % 8) * (N/16) + j / 8
-//   stage logN-2, entry N/4 + j  at slot  N/4 + (j % 4) * (N/16) + j / 4
-// for logN >= kTwPermMinLogN (the sizes of the cluster and batch kernels);
-// every other entry, and every entry of smaller tables, sits at its index.
+// stages every thread of the transform kernels owns a run of consecutive
+// entries (16, 8, 4, 2 of them in the last four stages with the usual 5-word
+// runs of a 4-stage register pass), so in the natural order the 32 lanes of a
+// warp would read 32 scattered cache lines per load.  The blocks of the last
+// four stages are therefore stored interleaved, which makes the lanes' loads
+// consecutive: for p = 0..3, stage logN-1-p's block starts at H = N / 2^(p+1)
+// and its entry H + j sits at slot
+//   H + (j % F) * (N/32) + j / F,   F = 16 / 2^p,
+// for logN >= kTwPermMinLogN (the sizes of the cluster and batch kernels,
+// whose last four stages are all in their second phase); every other entry,
+// and every entry of smaller tables, sits at its index.
 constexpr int kTwPermMinLogN = 10;
+constexpr int kTwPermStages = 4;
 NTT_HD constexpr uint32_t tw_slot(uint32_t i, int logN) {
     if (logN < kTwPermMinLogN) return i;
-    const uint32_t h = 1u << (logN - 1), qt = 1u << (logN - 2), s16 = 1u << (logN - 4);
-    if (i >= h) return h + ((i - h) & 7u) * s16 + ((i - h) >> 3);
-    if (i >= qt) return qt + ((i - qt) & 3u) * s16 + ((i - qt) >> 2);
+    const uint32_t s32 = 1u << (logN - 5);
+    for (int p = 0; p < kTwPermStages; ++p) {
+        const uint32_t h = 1u << (logN - 1 - p);
+        if (i >= h) {
+            const int lf = 4 - p;  // log2 F
+            return h + ((i - h) & ((1u << lf) - 1u)) * s32 + ((i - h) >> lf);
+        }
+    }
     return i;
 }
 

@@ -215,6 +215,8 @@ struct Geometry {
     static_assert(K1A >= 1 && K1A <= EB && K1B >= 0 && K1B <= EB, "phase-1 passes");
     static_assert(K2A >= 1 && K2A <= EB && K2B >= 0 && K2B <= EB, "phase-2 passes");
     static_assert(TB >= 5 && TB <= 10, "32..1024 threads per CTA");
+    static_assert(LOGN < kTwPermMinLogN || R2 >= kTwPermStages,
+                  "the interleaved twiddle stages must all lie in phase 2");
 
     // Bulk copies of the input slab in pieces of COPY_WORDS (<= 128 bytes, so
     // a piece never straddles a stage pad): forward = each phase-1 row's W1
@@ -325,9 +327,9 @@ struct Maps {
 // same butterfly of all NP polynomials of the job.
 // Perm != 0: the stage's twiddle block (starting at index H) is stored
 // interleaved by Perm (tw_slot, arith.cuh): entry H + j at slot
-// H + (j % Perm) * S16 + j / Perm.
+// H + (j % Perm) * S + j / Perm.
 template <class L, class Arith, bool Fwd, int k, bool Fold, int NP, int Perm = 0,
-          uint32_t H = 0, uint32_t S16 = 0, class Ctx>
+          uint32_t H = 0, uint32_t S = 0, class Ctx>
 NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
     constexpr int p = Fwd ? (L::PLO + L::KB - 1 - k) : (L::PLO + k);
     constexpr int gbits = Fwd ? k : (L::KB - 1 - k);
@@ -366,7 +368,7 @@ NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
                     w[0] = ctx.tw_ld(tb, 0);
                 }
             } else {
-                constexpr int lp = Perm == 8 ? 3 : 2;
+                constexpr int lp = Perm == 16 ? 4 : Perm == 8 ? 3 : Perm == 4 ? 2 : 1;
                 // the thread's part of the entry index, j0 = tbase - H, is a
                 // multiple of Perm when the lambda bits p+1 .. p+lp are
                 // register bits (zero in the thread's base): then the slot of
@@ -379,13 +381,13 @@ NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
                     ct_for<(1 << gbits)>([&](auto Gc) {
                         constexpr uint32_t c = xoff + decltype(Gc)::value;
                         w[decltype(Gc)::value] =
-                            ctx.tw_ld(tb, (c & (uint32_t)(Perm - 1)) * S16 + (c >> lp));
+                            ctx.tw_ld(tb, (c & (uint32_t)(Perm - 1)) * S + (c >> lp));
                     });
                 } else {
                     ct_for<(1 << gbits)>([&](auto Gc) {
                         const uint32_t j = j0 + xoff + decltype(Gc)::value;
                         w[decltype(Gc)::value] =
-                            ctx.tw_at(H + (j & (uint32_t)(Perm - 1)) * S16 + (j >> lp));
+                            ctx.tw_at(H + (j & (uint32_t)(Perm - 1)) * S + (j >> lp));
                     });
                 }
             }
@@ -427,13 +429,14 @@ NTT_HD void run_stages(Ctx& ctx, uint32_t (&v)[G::NP][L::E], uint32_t d) {
         constexpr bool s0 = HasStage0 && (Fwd ? (k == 0) : (k == L::KB - 1));
         const uint32_t tb =
             (Phase2 ? Mp::tw_base_p2(p, ctx.rank) : Mp::tw_base_p1(p)) + (d >> (p + 1));
-        // phase-2 bit 0 / 1 is the limb's stage logN-1 / logN-2, whose
-        // twiddles are stored interleaved (tw_slot)
-        constexpr bool kPermLayout = Phase2 && G::LOGN >= kTwPermMinLogN && p <= 1;
-        constexpr int perm = kPermLayout ? (p == 0 ? 8 : 4) : 0;
+        // phase-2 bit p < 4 is the limb's stage logN-1-p, whose twiddles are
+        // stored interleaved by 16 >> p (tw_slot)
+        constexpr bool kPermLayout =
+            Phase2 && G::LOGN >= kTwPermMinLogN && p < kTwPermStages;
+        constexpr int perm = kPermLayout ? (16 >> p) : 0;
         constexpr uint32_t h = kPermLayout ? (1u << (G::LOGN - 1 - p)) : 0u;
-        constexpr uint32_t s16 = kPermLayout ? (1u << (G::LOGN - 4)) : 0u;
-        stage<L, Arith, Fwd, k, s0, G::NP, perm, h, s16>(ctx, v, tb);
+        constexpr uint32_t s32 = kPermLayout ? (1u << (G::LOGN - 5)) : 0u;
+        stage<L, Arith, Fwd, k, s0, G::NP, perm, h, s32>(ctx, v, tb);
         if constexpr (ArriveAfterFirst && k == 0) ctx.after_local_reads();
     });
 }

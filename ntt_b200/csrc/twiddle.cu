@@ -13,8 +13,8 @@
 //                                         v04:567-580, folded into the last
 //                                         stage: N^-1 and from_mont)
 //            entry 1: psi^-bitrev(1) * c
-// Entry i is stored at slot tw_slot(i, logN) (arith.cuh): the last two stages'
-// blocks are interleaved for coalesced loads.
+// Entry i is stored at slot tw_slot(i, logN) (arith.cuh): the last four
+// stages' blocks are interleaved for coalesced loads.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "arith.cuh"

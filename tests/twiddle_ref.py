@@ -7,8 +7,9 @@ constants folded into limb stage 0:
   forward  [0] = R mod q, [1] = psi^bitrev(1) * R   (R = 2^32: Montgomery form)
   inverse  [0] = c = N^-1 * R^-1, [1] = psi^-bitrev(1) * c
 For logN >= 10 entry i is stored at slot tw_slot(i) below: the blocks of the
-last two stages are interleaved by 8 and 4 (entry N/2 + j at slot
-N/2 + (j % 8) * N/16 + j // 8; entry N/4 + j at N/4 + (j % 4) * N/16 + j // 4).
+last four stages are interleaved: stage logN-1-p (p = 0..3) starts at
+H = N / 2^(p+1) and its entry H + j sits at H + (j % F) * N/32 + j // F with
+F = 16 / 2^p.
 This module rebuilds that layout from the oracle so the CPU emulator and the
 GPU table check have an independent expected value.
 """
@@ -21,11 +22,10 @@ def tw_slot(i: int, logN: int) -> int:
     if logN < PERM_MIN_LOGN:
         return i
     N = 1 << logN
-    h, qt, s16 = N // 2, N // 4, N // 16
-    if i >= h:
-        return h + ((i - h) % 8) * s16 + (i - h) // 8
-    if i >= qt:
-        return qt + ((i - qt) % 4) * s16 + (i - qt) // 4
+    for p in range(4):
+        h, f = N >> (p + 1), 16 >> p
+        if i >= h:
+            return h + ((i - h) % f) * (N // 32) + (i - h) // f
     return i
 
 
