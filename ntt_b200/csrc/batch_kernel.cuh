@@ -165,6 +165,27 @@ struct BatchCtx {
     __device__ __forceinline__ uint32_t* s_base(uint32_t w) const { return smem + w; }
     __device__ __forceinline__ uint32_t s_ld(const uint32_t* b, uint32_t c) const { return b[c]; }
     __device__ __forceinline__ void s_st(uint32_t* b, uint32_t c, uint32_t v) const { b[c] = v; }
+    __device__ __forceinline__ void s_ld4(const uint32_t* b, uint32_t c, uint32_t& x, uint32_t& y,
+                                          uint32_t& z, uint32_t& w) const {
+        const uint4 t = *reinterpret_cast<const uint4*>(b + c);
+        x = t.x;
+        y = t.y;
+        z = t.z;
+        w = t.w;
+    }
+    __device__ __forceinline__ void s_st4(uint32_t* b, uint32_t c, uint32_t x, uint32_t y,
+                                          uint32_t z, uint32_t w) const {
+        *reinterpret_cast<uint4*>(b + c) = make_uint4(x, y, z, w);
+    }
+    __device__ __forceinline__ void s_ld2(const uint32_t* b, uint32_t c, uint32_t& x,
+                                          uint32_t& y) const {
+        const uint2 t = *reinterpret_cast<const uint2*>(b + c);
+        x = t.x;
+        y = t.y;
+    }
+    __device__ __forceinline__ void s_st2(uint32_t* b, uint32_t c, uint32_t x, uint32_t y) const {
+        *reinterpret_cast<uint2*>(b + c) = make_uint2(x, y);
+    }
     __device__ __forceinline__ auto r_base(uint32_t dst, uint32_t w) const {
         if constexpr (C == 1) {
             return smem + w;

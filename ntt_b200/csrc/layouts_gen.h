@@ -12,7 +12,7 @@ struct LayoutTable;
 
 template <>
 struct LayoutTable<10, 0, 5, 5, 5, 5> {
-    static constexpr int XW[5] = {5, 16, 6, 1, 1535};
+    static constexpr int XW[5] = {5, 4, 10, 0, 1148};
     static constexpr uint32_t lanes_P1A = 0x1fu;
     static constexpr uint32_t lanes_P1B = 0x3d0u;
     static constexpr uint32_t lanes_P2A = 0x3e0u;
@@ -21,7 +21,7 @@ struct LayoutTable<10, 0, 5, 5, 5, 5> {
 
 template <>
 struct LayoutTable<11, 0, 6, 5, 1, 5> {
-    static constexpr int XW[5] = {5, 1, 11, 0, 2111};
+    static constexpr int XW[5] = {5, 4, 11, 0, 2300};
     static constexpr uint32_t lanes_P1A = 0x1f0u;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x3e0u;
@@ -30,7 +30,7 @@ struct LayoutTable<11, 0, 6, 5, 1, 5> {
 
 template <>
 struct LayoutTable<12, 0, 7, 5, 3, 5> {
-    static constexpr int XW[5] = {5, 2, 9, 1, 4357};
+    static constexpr int XW[5] = {5, 4, 12, 0, 4604};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x21eu;
     static constexpr uint32_t lanes_P2A = 0x3e0u;
@@ -39,7 +39,7 @@ struct LayoutTable<12, 0, 7, 5, 3, 5> {
 
 template <>
 struct LayoutTable<12, 0, 6, 4, 3, 3> {
-    static constexpr int XW[5] = {1, 1, 6, 5, 6458};
+    static constexpr int XW[5] = {5, 4, 12, 0, 4604};
     static constexpr uint32_t lanes_P1A = 0x3eu;
     static constexpr uint32_t lanes_P1B = 0x3eu;
     static constexpr uint32_t lanes_P2A = 0x1c6u;
@@ -48,7 +48,7 @@ struct LayoutTable<12, 0, 6, 4, 3, 3> {
 
 template <>
 struct LayoutTable<13, 0, 8, 5, 3, 5> {
-    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
+    static constexpr int XW[5] = {5, 4, 13, 0, 9212};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x3e0u;
@@ -57,7 +57,7 @@ struct LayoutTable<13, 0, 8, 5, 3, 5> {
 
 template <>
 struct LayoutTable<14, 0, 9, 5, 4, 5> {
-    static constexpr int XW[5] = {5, 1, 14, 0, 16895};
+    static constexpr int XW[5] = {5, 4, 14, 0, 18428};
     static constexpr uint32_t lanes_P1A = 0x3eu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x3e0u;
@@ -66,7 +66,7 @@ struct LayoutTable<14, 0, 9, 5, 4, 5> {
 
 template <>
 struct LayoutTable<14, 1, 9, 5, 4, 5> {
-    static constexpr int XW[5] = {5, 1, 10, 16, 8559};
+    static constexpr int XW[5] = {5, 2, 9, 16, 8942};
     static constexpr uint32_t lanes_P1A = 0x3eu;
     static constexpr uint32_t lanes_P1B = 0x20fu;
     static constexpr uint32_t lanes_P2A = 0x3e0u;
@@ -75,7 +75,7 @@ struct LayoutTable<14, 1, 9, 5, 4, 5> {
 
 template <>
 struct LayoutTable<14, 1, 6, 6, 6, 4> {
-    static constexpr int XW[5] = {6, 4, 9, 1, 8715};
+    static constexpr int XW[5] = {6, 4, 13, 0, 8700};
     static constexpr uint32_t lanes_P1A = 0x1fu;
     static constexpr uint32_t lanes_P1B = 0x760u;
     static constexpr uint32_t lanes_P2A = 0x70cu;
@@ -93,7 +93,7 @@ struct LayoutTable<15, 1, 10, 5, 5, 5> {
 
 template <>
 struct LayoutTable<15, 2, 8, 5, 3, 4> {
-    static constexpr int XW[5] = {5, 1, 7, 8, 8951};
+    static constexpr int XW[5] = {5, 4, 13, 0, 9212};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x386u;
@@ -102,7 +102,7 @@ struct LayoutTable<15, 2, 8, 5, 3, 4> {
 
 template <>
 struct LayoutTable<15, 2, 6, 6, 6, 5> {
-    static constexpr int XW[5] = {5, 2, 6, 1, 8829};
+    static constexpr int XW[5] = {6, 4, 9, 16, 8940};
     static constexpr uint32_t lanes_P1A = 0x1fu;
     static constexpr uint32_t lanes_P1B = 0x760u;
     static constexpr uint32_t lanes_P2A = 0x60eu;
@@ -120,7 +120,7 @@ struct LayoutTable<16, 3, 8, 5, 3, 4> {
 
 template <>
 struct LayoutTable<16, 3, 7, 5, 3, 5> {
-    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
+    static constexpr int XW[5] = {6, 4, 9, 16, 8940};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x3eu;
     static constexpr uint32_t lanes_P2A = 0x20fu;
@@ -129,7 +129,7 @@ struct LayoutTable<16, 3, 7, 5, 3, 5> {
 
 template <>
 struct LayoutTable<16, 2, 8, 5, 3, 4> {
-    static constexpr int XW[5] = {5, 1, 6, 4, 17915};
+    static constexpr int XW[5] = {5, 4, 14, 0, 18428};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x30eu;
@@ -138,7 +138,7 @@ struct LayoutTable<16, 2, 8, 5, 3, 4> {
 
 template <>
 struct LayoutTable<16, 4, 8, 5, 3, 4> {
-    static constexpr int XW[5] = {5, 1, 12, 0, 4223};
+    static constexpr int XW[5] = {6, 4, 9, 16, 4460};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x20fu;
     static constexpr uint32_t lanes_P2A = 0x30eu;
@@ -147,7 +147,7 @@ struct LayoutTable<16, 4, 8, 5, 3, 4> {
 
 template <>
 struct LayoutTable<16, 3, 8, 4, 4, 4> {
-    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
+    static constexpr int XW[5] = {6, 4, 13, 0, 8700};
     static constexpr uint32_t lanes_P1A = 0x1fu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x10fu;
@@ -156,7 +156,7 @@ struct LayoutTable<16, 3, 8, 4, 4, 4> {
 
 template <>
 struct LayoutTable<16, 3, 6, 6, 6, 5> {
-    static constexpr int XW[5] = {6, 2, 10, 1, 8453};
+    static constexpr int XW[5] = {6, 4, 13, 0, 8700};
     static constexpr uint32_t lanes_P1A = 0x1fu;
     static constexpr uint32_t lanes_P1B = 0x760u;
     static constexpr uint32_t lanes_P2A = 0x41eu;
@@ -165,7 +165,7 @@ struct LayoutTable<16, 3, 6, 6, 6, 5> {
 
 template <>
 struct LayoutTable<16, 4, 6, 6, 6, 4> {
-    static constexpr int XW[5] = {5, 1, 10, 2, 4229};
+    static constexpr int XW[5] = {5, 2, 6, 2, 4476};
     static constexpr uint32_t lanes_P1A = 0x1fu;
     static constexpr uint32_t lanes_P1B = 0x7a0u;
     static constexpr uint32_t lanes_P2A = 0x43cu;
@@ -174,7 +174,7 @@ struct LayoutTable<16, 4, 6, 6, 6, 4> {
 
 template <>
 struct LayoutTable<16, 4, 8, 4, 4, 4> {
-    static constexpr int XW[5] = {5, 1, 8, 8, 4343};
+    static constexpr int XW[5] = {5, 2, 12, 0, 4350};
     static constexpr uint32_t lanes_P1A = 0x1fu;
     static constexpr uint32_t lanes_P1B = 0x10fu;
     static constexpr uint32_t lanes_P2A = 0x10fu;
@@ -183,7 +183,7 @@ struct LayoutTable<16, 4, 8, 4, 4, 4> {
 
 template <>
 struct LayoutTable<17, 3, 8, 5, 3, 5> {
-    static constexpr int XW[5] = {5, 1, 14, 0, 16895};
+    static constexpr int XW[5] = {6, 4, 9, 16, 17900};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x20fu;
@@ -192,7 +192,7 @@ struct LayoutTable<17, 3, 8, 5, 3, 5> {
 
 template <>
 struct LayoutTable<17, 4, 8, 5, 3, 5> {
-    static constexpr int XW[5] = {5, 1, 13, 0, 8447};
+    static constexpr int XW[5] = {6, 4, 9, 16, 8940};
     static constexpr uint32_t lanes_P1A = 0x7cu;
     static constexpr uint32_t lanes_P1B = 0x1fu;
     static constexpr uint32_t lanes_P2A = 0x20fu;
@@ -201,7 +201,7 @@ struct LayoutTable<17, 4, 8, 5, 3, 5> {
 
 template <>
 struct LayoutTable<17, 4, 6, 6, 6, 5> {
-    static constexpr int XW[5] = {5, 1, 10, 1, 8454};
+    static constexpr int XW[5] = {6, 4, 13, 0, 8700};
     static constexpr uint32_t lanes_P1A = 0x1fu;
     static constexpr uint32_t lanes_P1B = 0x760u;
     static constexpr uint32_t lanes_P2A = 0x3eu;

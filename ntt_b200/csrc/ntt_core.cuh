@@ -170,7 +170,23 @@ struct Spread {
     static constexpr uint32_t phys(uint32_t l) {
         return l + (uint32_t)C1 * (l >> A1) + (uint32_t)C2 * (l >> A2);
     }
+    // every aligned run of V lambdas maps to an aligned run of V words
+    template <int V>
+    static constexpr bool aligned() {
+        return C1 % V == 0 && C2 % V == 0 && (C1 == 0 || (1 << A1) % V == 0) &&
+               (C2 == 0 || (1 << A2) % V == 0);
+    }
 };
+
+// Width (words) of a pass's shared-memory accesses: 128-bit when the thread
+// owns runs of 4 consecutive lambdas and the layout keeps them aligned, else
+// 64-bit for runs of 2, else 32-bit (gen_layouts.py's vec_width).
+template <class L, class X>
+constexpr int smem_vec() {
+    if constexpr (L::kRunBits >= 2 && X::template aligned<4>()) return 4;
+    else if constexpr (L::kRunBits >= 1 && X::template aligned<2>()) return 2;
+    else return 1;
+}
 
 // Stage buffer: one 16-byte pad per 128 bytes (conflict-free 128-bit reads
 // whether a thread's run starts every 32 words or every row).
@@ -536,26 +552,50 @@ NTT_HD void load_input(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t d, uint32_t g
 }
 
 // Work buffer: polynomial p's slab starts Slab words after polynomial 0's.
+// The thread's base d is zero on its register bits, so with runs of V the
+// base and every run start are multiples of V (and so are their words).
 template <class L, class X, uint32_t Slab, int NP, class Ctx>
 NTT_HD void load_smem(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t d) {
+    constexpr int V = smem_vec<L, X>();
     auto sb = ctx.s_base(X::phys(d));
     ct_for<L::E>([&](auto R) {
         constexpr int r = decltype(R)::value;
+        constexpr uint32_t o = L::off(r);
         ct_for<NP>([&](auto Pp) {
             constexpr int pp = decltype(Pp)::value;
-            v[pp][r] = ctx.s_ld(sb, pp * Slab + X::phys(L::off(r)));
+            constexpr uint32_t c = pp * Slab + X::phys(o);
+            if constexpr (V == 1) {
+                v[pp][r] = ctx.s_ld(sb, c);
+            } else if constexpr ((o & (V - 1)) == 0) {
+                if constexpr (V == 4)
+                    ctx.s_ld4(sb, c, v[pp][L::reg_of(o)], v[pp][L::reg_of(o + 1)],
+                              v[pp][L::reg_of(o + 2)], v[pp][L::reg_of(o + 3)]);
+                else
+                    ctx.s_ld2(sb, c, v[pp][L::reg_of(o)], v[pp][L::reg_of(o + 1)]);
+            }
         });
     });
 }
 
 template <class L, class X, uint32_t Slab, int NP, class Ctx>
 NTT_HD void store_smem(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t d) {
+    constexpr int V = smem_vec<L, X>();
     auto sb = ctx.s_base(X::phys(d));
     ct_for<L::E>([&](auto R) {
         constexpr int r = decltype(R)::value;
+        constexpr uint32_t o = L::off(r);
         ct_for<NP>([&](auto Pp) {
             constexpr int pp = decltype(Pp)::value;
-            ctx.s_st(sb, pp * Slab + X::phys(L::off(r)), v[pp][r]);
+            constexpr uint32_t c = pp * Slab + X::phys(o);
+            if constexpr (V == 1) {
+                ctx.s_st(sb, c, v[pp][r]);
+            } else if constexpr ((o & (V - 1)) == 0) {
+                if constexpr (V == 4)
+                    ctx.s_st4(sb, c, v[pp][L::reg_of(o)], v[pp][L::reg_of(o + 1)],
+                              v[pp][L::reg_of(o + 2)], v[pp][L::reg_of(o + 3)]);
+                else
+                    ctx.s_st2(sb, c, v[pp][L::reg_of(o)], v[pp][L::reg_of(o + 1)]);
+            }
         });
     });
 }
@@ -631,28 +671,42 @@ NTT_HD void scatter_regs(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t dd, uint32_
 // 128-byte line.  A register pass's own accesses would put each lane on its
 // own line (a thread holds runs of consecutive words), which costs the L1
 // pipe 32 wavefronts per instruction instead of one to four.
+// With a layout that keeps 4-word runs aligned, lane l moves the 16-byte
+// pieces 4l, 4l + 128, ... instead (one line per quarter warp).
 template <class G>
 struct SlabChunk {
     static constexpr uint32_t WARPS = G::THREADS / 32u;
     static constexpr uint32_t WORDS = G::M / WARPS;
-    static_assert(WORDS % 32u == 0, "warp chunks of whole lines");
-    // lambda of lane 0 of this warp's chunk plus the lane (bit-disjoint from
-    // the per-step offsets 32 * i, so phys() splits into base + immediate)
-    NTT_HD static uint32_t base(uint32_t tid) { return (tid >> 5) * WORDS + (tid & 31u); }
+    static constexpr bool VEC = G::XW::template aligned<4>();
+    static constexpr uint32_t STEP = VEC ? 128u : 32u;  // words per warp step
+    static_assert(WORDS % STEP == 0, "warp chunks of whole lines");
+    // lambda of this lane's first word (bit-disjoint from the per-step
+    // offsets STEP * i, so phys() splits into base + immediate)
+    NTT_HD static uint32_t base(uint32_t tid) {
+        return (tid >> 5) * WORDS + (VEC ? 4u : 1u) * (tid & 31u);
+    }
 };
 
 // Work buffer -> global: the slab's canonical words, stored through the
 // context's o_* interface (plain store, or the product epilogue).
 template <class G, class X, class Ctx>
 NTT_HD void slab_out(Ctx& ctx, uint32_t tid) {
-    const uint32_t b = SlabChunk<G>::base(tid);
+    using SC = SlabChunk<G>;
+    const uint32_t b = SC::base(tid);
     auto sb = ctx.s_base(X::phys(b));
     ct_for<G::NP>([&](auto Pp) {
         constexpr int pp = decltype(Pp)::value;
         auto gb = ctx.o_base(pp, b + ctx.rank * G::M);
-        ct_for<SlabChunk<G>::WORDS / 32u>([&](auto I) {
-            constexpr uint32_t o = 32u * decltype(I)::value;
-            ctx.o_st(gb, o, ctx.s_ld(sb, pp * G::SLAB_WORDS + X::phys(o)));
+        ct_for<SC::WORDS / SC::STEP>([&](auto I) {
+            constexpr uint32_t o = SC::STEP * decltype(I)::value;
+            constexpr uint32_t c = pp * G::SLAB_WORDS + X::phys(o);
+            if constexpr (SC::VEC) {
+                uint32_t x, y, z, w;
+                ctx.s_ld4(sb, c, x, y, z, w);
+                ctx.o_st4(gb, o, x, y, z, w);
+            } else {
+                ctx.o_st(gb, o, ctx.s_ld(sb, c));
+            }
         });
     });
 }
@@ -660,18 +714,28 @@ NTT_HD void slab_out(Ctx& ctx, uint32_t tid) {
 // Global -> work buffer: the inverse's input slab.
 template <class G, class X, class Ctx>
 NTT_HD void slab_in(Ctx& ctx, uint32_t tid) {
-    const uint32_t b = SlabChunk<G>::base(tid);
+    using SC = SlabChunk<G>;
+    constexpr uint32_t K = SC::WORDS / SC::STEP, V = SC::VEC ? 4u : 1u;
+    const uint32_t b = SC::base(tid);
     auto sb = ctx.s_base(X::phys(b));
     ct_for<G::NP>([&](auto Pp) {
         constexpr int pp = decltype(Pp)::value;
         auto gb = ctx.g_base(pp, b + ctx.rank * G::M);
-        uint32_t w[SlabChunk<G>::WORDS / 32u];
-        ct_for<SlabChunk<G>::WORDS / 32u>([&](auto I) {
-            w[decltype(I)::value] = ctx.g_ld(gb, 32u * decltype(I)::value);
+        uint32_t w[K * V];
+        ct_for<K>([&](auto I) {
+            constexpr uint32_t i = decltype(I)::value;
+            if constexpr (SC::VEC)
+                ctx.g_ld4(gb, SC::STEP * i, w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+            else
+                w[i] = ctx.g_ld(gb, SC::STEP * i);
         });
-        ct_for<SlabChunk<G>::WORDS / 32u>([&](auto I) {
-            constexpr uint32_t o = 32u * decltype(I)::value;
-            ctx.s_st(sb, pp * G::SLAB_WORDS + X::phys(o), w[decltype(I)::value]);
+        ct_for<K>([&](auto I) {
+            constexpr uint32_t i = decltype(I)::value;
+            constexpr uint32_t c = pp * G::SLAB_WORDS + X::phys(SC::STEP * i);
+            if constexpr (SC::VEC)
+                ctx.s_st4(sb, c, w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+            else
+                ctx.s_st(sb, c, w[i]);
         });
     });
 }

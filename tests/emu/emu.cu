@@ -15,15 +15,17 @@ void account(EmuCluster& cl, Stats& st) {
     std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>, std::vector<uint32_t>>
         groups;
     for (auto& a : cl.log) groups[{a.src, a.warp, a.seq, a.kind, a.rank_dst}].push_back(a.addr);
-    double worst_step = 0, sum_step = 0, wk[4] = {0, 0, 0, 0};
+    double worst_step = 0, sum_step = 0, wk[6] = {0, 0, 0, 0, 0, 0};
     long n_step = 0;
     for (auto& kv : groups) {
         const uint32_t kd = std::get<3>(kv.first);
-        const bool vec = kd == 3;
+        // 16-byte pieces (stage reads, kind 3; 128-bit work-buffer accesses,
+        // kind 4) in groups of 4 banks, 8-byte pieces (kind 5) in pairs
+        const uint32_t vw = (kd == 3 || kd == 4) ? 4u : kd == 5 ? 2u : 1u;
         std::map<uint32_t, std::vector<uint32_t>> banks;
         for (uint32_t w0 : kv.second) {
-            const uint32_t w = vec ? w0 / 4 : w0;
-            auto& v = banks[vec ? (w % 8) : (w % 32)];
+            const uint32_t w = w0 / vw;
+            auto& v = banks[w % (32u / vw)];
             bool dup = false;
             for (uint32_t x : v) dup |= (x == w);
             if (!dup) v.push_back(w);

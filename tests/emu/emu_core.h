@@ -30,7 +30,7 @@ namespace emu {
 
 
 struct Access {
-    uint32_t warp, seq, kind, rank_dst;  // kind: 0 lds, 1 sts, 2 dsmem, 3 stage128
+    uint32_t warp, seq, kind, rank_dst;  // kind: 0 lds, 1 sts, 2 dsmem, 3 stage128, 4 / 5 work buffer 128 / 64-bit (rank_dst: the warp phase)
     uint32_t addr;
     uint32_t src;  // issuing CTA
 };
@@ -168,6 +168,46 @@ struct EmuCtx {
         cl->smem[rank][w] = v;
         cl->writer[rank][w] = tid / 32;
         cl->writes[rank][w]++;
+    }
+    // 64- / 128-bit accesses: aligned, each word checked as a scalar one;
+    // logged once per warp phase (kind 4: 16-byte pieces per quarter warp,
+    // kind 5: 8-byte pieces per half warp) for the conflict accounting
+    void s_vec(uint32_t b, uint32_t c, uint32_t* v, int n, bool store) {
+        const uint32_t w = b + c;
+        if (w % (uint32_t)n || w + n - 1 >= cl->smem_words) {
+            fail(store ? "vector s_st out of range or misaligned" : "vector s_ld out of range or misaligned", w);
+            return;
+        }
+        cl->log.push_back({tid / 32, seq++, n == 4 ? 4u : 5u, (tid % 32) / (n == 4 ? 8u : 16u), w, rank});
+        for (int k = 0; k < n; ++k) {
+            if (store) {
+                cl->smem[rank][w + k] = v[k];
+                cl->writer[rank][w + k] = tid / 32;
+                cl->writes[rank][w + k]++;
+            } else {
+                if (cl->warp_local && cl->writer[rank][w + k] != tid / 32)
+                    fail("warp-local read of another warp's word", w + k);
+                v[k] = cl->smem[rank][w + k];
+            }
+        }
+    }
+    void s_ld4(uint32_t b, uint32_t c, uint32_t& x, uint32_t& y, uint32_t& z, uint32_t& w4) {
+        uint32_t v[4] = {0, 0, 0, 0};
+        s_vec(b, c, v, 4, false);
+        x = v[0], y = v[1], z = v[2], w4 = v[3];
+    }
+    void s_st4(uint32_t b, uint32_t c, uint32_t x, uint32_t y, uint32_t z, uint32_t w4) {
+        uint32_t v[4] = {x, y, z, w4};
+        s_vec(b, c, v, 4, true);
+    }
+    void s_ld2(uint32_t b, uint32_t c, uint32_t& x, uint32_t& y) {
+        uint32_t v[2] = {0, 0};
+        s_vec(b, c, v, 2, false);
+        x = v[0], y = v[1];
+    }
+    void s_st2(uint32_t b, uint32_t c, uint32_t x, uint32_t y) {
+        uint32_t v[2] = {x, y};
+        s_vec(b, c, v, 2, true);
     }
     std::pair<uint32_t, uint32_t> r_base(uint32_t dst, uint32_t w) { return {dst, w}; }
     template <uint32_t Off>
