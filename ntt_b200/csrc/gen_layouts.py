@@ -203,8 +203,9 @@ def search(MB, passes, scalar_pats, chunk_words):
 
 # Layouts kept by measurement on B200 where the cost model's choice was slower:
 # the forward default (2^16, 8-CTA cluster, R1 = 8) runs 0.250 ms per 64 x 16
-# limbs with its scalar layout and 0.262 ms with the vector-aligned one the
-# model prefers.
+# limbs with its scalar layout, 0.262 ms with the vector-aligned one the model
+# prefers (6, 4, 13, 0) and 0.264 ms with (5, 4, 13, 0), whose 128-bit
+# accesses are conflict-free but whose 64-bit phase-2 accesses are 2-way.
 MEASURED = {(16, 3, 8, 5, 3, 4): (5, 1, 13, 0)}
 
 
