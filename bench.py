@@ -189,16 +189,45 @@ def max_over_ranks(value_ms: float, device: str = "cuda") -> float:
     return float(t.item())
 
 
+def rank_env():
+    """(world, rank, local rank) from the launcher's environment."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def relaunch_under_torchrun(gpus: int) -> int:
+    """`--gpus N` (N > 1) started as a plain process: run this same command
+    line as N ranks under torch.distributed.run (one process per GPU,
+    rendezvous on 127.0.0.1) and return its exit status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={gpus}", "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def init_ranks(args, backend="nccl"):
+    """Join the process group of a multi-rank run (short timeout, so that a
+    rank that never arrives ends the others' waits with an error); the
+    world size must be the `--gpus` asked for."""
+    import datetime
+    import torch.distributed as dist
+    world, rank, local = rank_env()
+    if world != args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}")
+    if world > 1:
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    world, rank, local = init_ranks(args)
     torch.cuda.set_device(local)
     import ntt_b200 as nb
 
@@ -641,6 +670,8 @@ def bench_serve(args, torch, nb):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch_under_torchrun(args.gpus))
     if args.impl == "reference":
         run_reference(args)
     else:

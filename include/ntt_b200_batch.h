@@ -100,8 +100,12 @@ NTT_API ntt_status_t ntt_batch_submit(const ntt_job_t* jobs, int count, ntt_stre
  * them on one stream or wait between them -- overlapping calls race.  The
  * scratch's group counter must be zero at kernel start; each call zeroes it
  * on `stream` itself.  The first call on a device looks up the scratch's
- * address (one-time set-up); make it before any stream capture.  Does not
- * wait for the kernel. */
+ * address (one-time set-up); make it before any stream capture.  The
+ * descriptors are staged through one host area that the next call
+ * overwrites, so a call on a stream that is capturing a graph returns
+ * NTT_ERR_UNSUPPORTED.  The call keeps pointers to the resident tables
+ * without holding them: do not call ntt_tables_trim while calls are in
+ * flight.  Does not wait for the kernel. */
 #define NTT_NOALLOC_MAX_TILES 4096
 NTT_API ntt_status_t ntt_batch_run_noalloc(const ntt_job_t* jobs, int count, ntt_stream_t stream);
 

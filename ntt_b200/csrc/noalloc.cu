@@ -24,6 +24,12 @@
 //  * the first call on each device looks the scratch's device address up
 //    (cudaGetSymbolAddress, which may load this file's device code); make
 //    that first call before any stream capture;
+//  * the descriptors are staged through one static host area that the next
+//    call overwrites, so a call on a stream that is being captured into a
+//    graph is refused (NTT_ERR_UNSUPPORTED): a captured copy would read that
+//    area again at every replay, by then holding another call's descriptors;
+//  * the call keeps raw pointers to the registry's tables without holding
+//    them, so ntt_tables_trim must not run while calls are in flight;
 //  * the descriptors are staged through pageable host memory, so the call
 //    returns once earlier work on `stream` has drained far enough for the
 //    driver to take the copy.
@@ -141,6 +147,13 @@ extern "C" ntt_status_t ntt_batch_run_noalloc(const ntt_job_t* jobs, int count,
     if (cudaGetDevice(&dev) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaGetDevice");
     const int cl = max_logn >= 17 ? 16 : 8;
     const cudaStream_t s = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaError_t e = cudaStreamIsCapturing(s, &cap); e != cudaSuccess)
+        return cuda_fail(e, "cudaStreamIsCapturing");
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(NTT_ERR_UNSUPPORTED,
+                    "the allocation-free entry point stages its descriptors in one host area "
+                    "that the next call overwrites; it cannot run on a capturing stream");
 
     std::lock_guard<std::mutex> lk(g_mu);
     unsigned char* scratch = nullptr;

@@ -41,12 +41,19 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_u32p)
 
 
+def ref_root() -> str:
+    """The reference checkout: $NTT_REF_ROOT when set, else its location in
+    the build container (absent on machines that only run the prebuilt
+    harness)."""
+    return os.environ.get("NTT_REF_ROOT", "/root/reference")
+
+
 def build() -> None:
     """Compile liboracle.so (and the reference harness when the reference
     checkout is present)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if os.path.isdir(os.path.join(ref_root(), "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={ref_root()}"], check=True)
 
 
 def lib() -> ctypes.CDLL:
