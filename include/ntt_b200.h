@@ -128,6 +128,8 @@ typedef struct ntt_plan_info {
     TransformConfig effective; /* the phase triples the kernels run          */
     size_t device_bytes;    /* twiddle tables + constants held by the plan  */
     int tuned;              /* 1 if the configuration came from the tuner   */
+    int fwd_config;         /* catalogue index (ntt_config_get) of the      */
+    int inv_config;         /* forward / inverse kernel; -1: small sizes    */
 } ntt_plan_info_t;
 
 /* Validates every (qi, primitive_root) exactly as make_modulus_runtime does
@@ -161,6 +163,23 @@ NTT_API ntt_status_t ntt_forward_many(const ntt_plan_t* plan, uint32_t* a_dev, s
                               size_t poly_stride, ntt_stream_t stream);
 NTT_API ntt_status_t ntt_inverse_many(const ntt_plan_t* plan, uint32_t* a_dev, size_t polys,
                               size_t poly_stride, ntt_stream_t stream);
+/* Transforms with a per-limb constant folded in, at no extra launch or pass
+ * (Cheddar's NTTHandler multiplies by a per-limb constant inside its
+ * transform kernels: the pre-multiply of NTTPhase1, src/NTT_cheddar.cu:286-293,
+ * and INTTAndMultConst, src/NTT_cheddar.cu:743-813):
+ *   ntt_forward_scaled: a <- NTT(c_l * a) per limb l;
+ *   ntt_inverse_scaled: a <- c_l * INTT(a) per limb l.
+ * scale: device array of `limbs` uint32 constants, normal domain (reduced
+ * mod q_l).  The constant enters through the limb's stage-0 twiddle pair
+ * (table entries 0 and 1, which already carry the Montgomery and N^{-1}
+ * factors), so the cost is that of the plain transform.  Same layout,
+ * alignment and polys / poly_stride rules as ntt_forward_many. */
+NTT_API ntt_status_t ntt_forward_scaled(const ntt_plan_t* plan, uint32_t* a_dev, size_t polys,
+                                        size_t poly_stride, const uint32_t* scale_dev,
+                                        ntt_stream_t stream);
+NTT_API ntt_status_t ntt_inverse_scaled(const ntt_plan_t* plan, uint32_t* a_dev, size_t polys,
+                                        size_t poly_stride, const uint32_t* scale_dev,
+                                        ntt_stream_t stream);
 /* c = a (.) b: pointwise Montgomery product of two forward outputs (x*2^32
  * domain) per limb modulus, giving the spectrum of the negacyclic product
  * for ntt_inverse.  Over `polys` polynomials (poly_stride words apart, 0 =

@@ -58,6 +58,14 @@ NTT_API ntt_status_t ntt_plan_force_config(ntt_plan_t* plan, int fwd_index, int 
 /* Work distribution of the plan's launches (NTT_SCHEDULE_*; default
  * NTT_SCHEDULE_DIRECT). */
 NTT_API ntt_status_t ntt_plan_set_schedule(ntt_plan_t* plan, int schedule);
+/* Self-test of the kernels' failure detection (no reference counterpart):
+ * runs, on `stream`, the bounded mbarrier wait the transform kernels use,
+ * on a barrier that nothing ever completes, with a limit of `limit` tries
+ * (1..65536).  The wait gives up, the kernel returns normally and the
+ * expiry is recorded in the plan's status word, so that the following
+ * ntt_plan_check returns NTT_ERR_TIMEOUT.  The context stays usable. */
+NTT_API ntt_status_t ntt_selftest_wait_expiry(const ntt_plan_t* plan, uint32_t limit,
+                                              ntt_stream_t stream);
 /* Drop tuned entries for this process (plans fall back to defaults). */
 NTT_API void ntt_autotune_forget(void);
 /* Re-read the cache file on next use. */

@@ -80,7 +80,7 @@ class PlanInfo(ctypes.Structure):
     _fields_ = [("logN", ctypes.c_int), ("limbs", ctypes.c_int), ("cluster_ctas", ctypes.c_int),
                 ("threads_per_cta", ctypes.c_int), ("smem_bytes", ctypes.c_uint32),
                 ("effective", TransformConfig), ("device_bytes", ctypes.c_size_t),
-                ("tuned", ctypes.c_int)]
+                ("tuned", ctypes.c_int), ("fwd_config", ctypes.c_int), ("inv_config", ctypes.c_int)]
 
 
 class KernelConfig(ctypes.Structure):
@@ -166,6 +166,9 @@ _sig("ntt_config_resident_clusters", ctypes.c_int, ctypes.c_int, ctypes.c_int, c
 SCHEDULE_DIRECT = 0
 SCHEDULE_STAGED = 1
 _sig("ntt_autotune_reload", None)
+_sig("ntt_selftest_wait_expiry", _st, _vp, ctypes.c_uint32, _vp)
+_sig("ntt_forward_scaled", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp, _vp)
+_sig("ntt_inverse_scaled", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp, _vp)
 
 
 def _check(st: int, where: str):
@@ -318,6 +321,13 @@ class Plan:
         _check(_lib.ntt_plan_check(self._h, ctypes.byref(st)), "ntt_plan_check")
         return st.value
 
+    def selftest_wait_expiry(self, limit: int = 256, stream=None):
+        """Run the kernels' bounded mbarrier wait on a barrier nothing
+        completes (gives up after `limit` tries); the next check() raises
+        NttError(NTT_ERR_TIMEOUT)."""
+        _check(_lib.ntt_selftest_wait_expiry(self._h, limit, _stream(stream)),
+               "ntt_selftest_wait_expiry")
+
     def tables(self):
         """(forward pairs, inverse pairs, moduli) device addresses."""
         f, i, q = _vp(), _vp(), _vp()
@@ -338,6 +348,17 @@ class Plan:
     def inverse_many(self, a, polys: int, poly_stride: int = 0, stream=None):
         _check(_lib.ntt_inverse_many(self._h, _ptr(a), polys, poly_stride, _stream(stream)),
                "ntt_inverse_many")
+
+    def forward_scaled(self, a, scale, polys: int = 1, poly_stride: int = 0, stream=None):
+        """a <- NTT(c_l * a) per limb l; `scale`: device array of one uint32
+        constant per limb (normal domain)."""
+        _check(_lib.ntt_forward_scaled(self._h, _ptr(a), polys, poly_stride, _ptr(scale),
+                                       _stream(stream)), "ntt_forward_scaled")
+
+    def inverse_scaled(self, a, scale, polys: int = 1, poly_stride: int = 0, stream=None):
+        """a <- c_l * INTT(a) per limb l (see forward_scaled)."""
+        _check(_lib.ntt_inverse_scaled(self._h, _ptr(a), polys, poly_stride, _ptr(scale),
+                                       _stream(stream)), "ntt_inverse_scaled")
 
     def pointwise_mul(self, c, a, b, polys: int = 1, poly_stride: int = 0, stream=None):
         """c = a (.) b: Montgomery product of two forward outputs per limb."""

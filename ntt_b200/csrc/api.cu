@@ -524,6 +524,8 @@ ntt_status_t ntt_plan_get_info(const ntt_plan_t* p, ntt_plan_info_t* out) {
     out->effective = p->effective;
     out->device_bytes = p->bytes;
     out->tuned = p->tuned;
+    out->fwd_config = p->cfg_fwd ? (int)(p->cfg_fwd - fused_configs()) : -1;
+    out->inv_config = p->cfg_inv ? (int)(p->cfg_inv - fused_configs()) : -1;
     return NTT_OK;
 }
 
@@ -557,6 +559,30 @@ ntt_status_t ntt_plan_check(const ntt_plan_t* p, uint32_t* device_status) {
     return NTT_OK;
 }
 
+// The transform kernels' bounded mbarrier wait, run on a barrier that no
+// thread arrives on and no copy completes: it gives up after `limit` tries
+// and records the expiry in the status word exactly as the kernels do.
+__global__ void wait_expiry_kernel(uint32_t* status, uint32_t limit) {
+    __shared__ __align__(8) unsigned long long bar;
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(&bar);
+    if (threadIdx.x == 0) {
+        mbar_init(sa, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(sa, 0u, limit);
+    if (!ok && threadIdx.x == 0 && status) atomicOr(status, kStatusWaitExpired);
+}
+
+ntt_status_t ntt_selftest_wait_expiry(const ntt_plan_t* p, uint32_t limit, ntt_stream_t stream) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    if (limit == 0 || limit > (1u << 16))
+        return fail(NTT_ERR_INVALID_ARGUMENT, "limit must be in [1, 65536] tries");
+    wait_expiry_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(p->status, limit);
+    NTT_CUDA_TRY(cudaGetLastError(), "wait-expiry launch");
+    return NTT_OK;
+}
+
 ntt_status_t ntt_plan_set_schedule(ntt_plan_t* p, int schedule) {
     if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
     if (schedule != NTT_SCHEDULE_DIRECT && schedule != NTT_SCHEDULE_STAGED)
@@ -584,7 +610,7 @@ namespace nttb {
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
                            cudaStream_t s, uint32_t* status, int schedule, bool lazy2,
-                           const uint32_t* mul_src) {
+                           const uint32_t* mul_src, const uint32_t* scale) {
     if (polys == 0) return NTT_OK;
     if (!a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL data pointer");
     if (mul_src && (!cfg || !fwd))
@@ -606,16 +632,18 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
         return fail(NTT_ERR_INVALID_ARGUMENT, "too many limbs");
     if (cfg) {
         FusedArgs fa{a,  tw, q, (uint32_t)limbs, (uint32_t)polys, (uint32_t)jobs, 1u,
-                     (unsigned long long)stride, status, mul_src, (unsigned long long)stride};
+                     (unsigned long long)stride, status, mul_src, (unsigned long long)stride,
+                     scale};
         return launch_fused(cfg, fwd, fa, s, schedule, lazy2, mul_src != nullptr);
     }
-    SmallArgs sa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride, logN};
+    SmallArgs sa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride, logN,
+                 scale};
     NTT_CUDA_TRY(launch_small(sa, fwd, s), "small NTT launch");
     return NTT_OK;
 }
 
 static ntt_status_t plan_run(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
-                             bool fwd, ntt_stream_t s) {
+                             bool fwd, ntt_stream_t s, const uint32_t* scale = nullptr) {
     if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
     int dev = 0;
     NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
@@ -627,7 +655,7 @@ static ntt_status_t plan_run(const ntt_plan_t* p, uint32_t* a, size_t polys, siz
     if (cfg && (polys == 1 || polys < (size_t)cfg->np)) cfg = fwd ? p->cfg_fwd1 : p->cfg_inv1;
     return run_transform(p->logN, cfg, fwd ? p->fwd : p->inv, p->q,
                          p->limbs, a, polys, stride, fwd, (cudaStream_t)s, p->status,
-                         p->schedule, p->lazy2);
+                         p->schedule, p->lazy2, nullptr, scale);
 }
 
 }  // namespace nttb
@@ -647,6 +675,17 @@ ntt_status_t ntt_forward_many(const ntt_plan_t* p, uint32_t* a, size_t polys, si
 ntt_status_t ntt_inverse_many(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
                               ntt_stream_t s) {
     return plan_run(p, a, polys, stride, false, s);
+}
+
+ntt_status_t ntt_forward_scaled(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
+                                const uint32_t* scale, ntt_stream_t s) {
+    if (!scale) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL scale array");
+    return plan_run(p, a, polys, stride, true, s, scale);
+}
+ntt_status_t ntt_inverse_scaled(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
+                                const uint32_t* scale, ntt_stream_t s) {
+    if (!scale) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL scale array");
+    return plan_run(p, a, polys, stride, false, s, scale);
 }
 
 ntt_status_t ntt_pointwise_mul(const ntt_plan_t* p, uint32_t* c, const uint32_t* a,

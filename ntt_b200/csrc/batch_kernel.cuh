@@ -211,6 +211,8 @@ struct BatchCtx {
         const uint2 t = __ldg(reinterpret_cast<const uint2*>(twp) + i);
         return TwPair{t.x, t.y};
     }
+    // table entries 0 and 1 (the constants folded into the limb's stage 0)
+    __device__ __forceinline__ TwPair fold_at(uint32_t i) const { return tw_at(i); }
     __device__ __forceinline__ const TwPair* tw_base(uint32_t i) const { return twp + i; }
     __device__ __forceinline__ TwPair tw_ld(const TwPair* b, uint32_t c) const {
         const uint2 t = __ldg(reinterpret_cast<const uint2*>(b + c));

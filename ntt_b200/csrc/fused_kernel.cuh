@@ -32,7 +32,18 @@ struct FusedArgs {
     uint32_t* status;  // optional: bit 0 set when a bounded wait expired
     const uint32_t* src;  // Mul only: the forward's input
     unsigned long long src_stride;
+    // optional per-limb constants c (normal domain): the forward transforms
+    // c * x, the inverse returns c * INTT(x), both folded into stage 0
+    const uint32_t* scale;
 };
+
+// The constant table entry t times c, with its Shoup companion (computed
+// once per thread per job: two 64-bit divisions by q).
+__device__ __forceinline__ TwPair scaled_pair(TwPair t, uint32_t c, uint32_t q) {
+    const uint32_t w = (uint32_t)(((unsigned long long)t.w * c) % q);
+    return TwPair{w, (uint32_t)(((unsigned long long)w << 32) / q)};
+}
+constexpr uint32_t kNoScale = 0xFFFFFFFFu;
 
 // -q^{-1} mod 2^32 by Newton's iteration (q odd: q is its own inverse mod 8).
 __device__ __forceinline__ uint32_t neg_qinv_dev(uint32_t q) {
@@ -95,9 +106,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t sa, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: false when kWaitLimit tries expired.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t sa, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
+// Bounded wait: false when `limit` tries expired.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t sa, uint32_t parity,
+                                                  uint32_t limit = kWaitLimit) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(sa, parity)) return true;
     return false;
 }
@@ -130,6 +142,7 @@ struct DevCtx {
     const uint32_t* stage;  // padded copy of this CTA's input slab (staged)
     uint32_t smem_sa;       // .shared window address of smem
     uint32_t q, q2, rank;
+    uint32_t scale_c = kNoScale;  // this job's limb constant (kNoScale: none)
 
     // global data (direct input): L1-cached, because a thread owning a
     // contiguous run reads each 32-byte sector in two 16-byte halves
@@ -227,6 +240,12 @@ struct DevCtx {
     __device__ __forceinline__ TwPair tw_at(uint32_t i) const {
         const uint2 t = __ldg(reinterpret_cast<const uint2*>(twp) + i);
         return TwPair{t.x, t.y};
+    }
+    // table entries 0 and 1 (the constants folded into the limb's stage 0),
+    // times the job's limb constant when the launch carries one
+    __device__ __forceinline__ TwPair fold_at(uint32_t i) const {
+        const TwPair t = tw_at(i);
+        return scale_c == kNoScale ? t : scaled_pair(t, scale_c, q);
     }
     __device__ __forceinline__ const TwPair* tw_base(uint32_t i) const { return twp + i; }
     __device__ __forceinline__ TwPair tw_ld(const TwPair* b, uint32_t c) const {
@@ -382,6 +401,7 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedA
         ctx.twp = a.tw + ((size_t)limb << G::LOGN);
         ctx.q = __ldg(a.q + limb);
         ctx.q2 = 2u * ctx.q;
+        if (a.scale) ctx.scale_c = __ldg(a.scale + limb) % ctx.q;
         if constexpr (Mul) ctx.qinv = neg_qinv_dev(ctx.q);
         if constexpr (Staged) {
             if (!mbar_wait_bounded(mbar_sa, parity) && a.status)

@@ -356,7 +356,7 @@ NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
     const uint32_t q = ctx.q, q2 = ctx.q2;
     if constexpr (Fold) {
         static_assert(gbits == 0, "stage 0 of the limb has a single group");
-        const TwPair f = ctx.tw_at(0u), w = ctx.tw_at(1u);
+        const TwPair f = ctx.fold_at(0u), w = ctx.fold_at(1u);
         ct_for<(L::E >> 1)>([&](auto I) {
             constexpr int i = decltype(I)::value;
             // the E/2 pairs: the lower register has bit (bbit + XB) clear

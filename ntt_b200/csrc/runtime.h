@@ -38,9 +38,11 @@ ntt_status_t twiddle_gen_inputs(int logN, ModulusConfig m, TwGenLimb* fwd, TwGen
 // mul_src (fused forward only): transform mul_src (same shape and stride)
 // instead and store the Montgomery product of each output word with the
 // spectrum word already at its place in `a`.
+// scale (optional, device, one constant per limb): forward of c * x, or
+// c * inverse, folded into the limb's stage 0.
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
                            cudaStream_t s, uint32_t* status, int schedule, bool lazy2,
-                           const uint32_t* mul_src = nullptr);
+                           const uint32_t* mul_src = nullptr, const uint32_t* scale = nullptr);
 
 }  // namespace nttb

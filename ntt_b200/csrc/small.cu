@@ -8,8 +8,17 @@
 
 namespace nttb {
 
+// Table entry t times c (normal domain) with its Shoup companion.
+__device__ __forceinline__ TwPair small_scaled(TwPair t, uint32_t c, uint32_t q) {
+    const uint32_t w = (uint32_t)(((unsigned long long)t.w * c) % q);
+    return TwPair{w, (uint32_t)(((unsigned long long)w << 32) / q)};
+}
+
+// f0, f1: table entries 0 and 1 (the constants folded into stage 0), already
+// scaled by the launch's limb constant if it carries one.
 template <class Arith, bool Fwd>
-__device__ void small_body(uint32_t* a, const TwPair* tw, uint32_t q, int logN, uint32_t* s) {
+__device__ void small_body(uint32_t* a, const TwPair* tw, uint32_t q, int logN, uint32_t* s,
+                           TwPair f0, TwPair f1) {
     const uint32_t N = 1u << logN, half = N >> 1, q2 = 2u * q;
     for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) s[i] = a[i];
     __syncthreads();
@@ -21,13 +30,13 @@ __device__ void small_body(uint32_t* a, const TwPair* tw, uint32_t q, int logN, 
             const uint32_t j = b / t, k = j * 2 * t + (b % t);
             uint32_t x = s[k], y = s[k + t];
             if (Fwd) {
-                if (sg == 0) Arith::ct_first(x, y, tw[0], tw[1], q, q2);
+                if (sg == 0) Arith::ct_first(x, y, f0, f1, q, q2);
                 else {
                     const TwPair w = tw[(1u << sg) + j];
                     Arith::ct(x, y, w.w, w.wp, q, q2);
                 }
             } else {
-                if (sg == 0) Arith::gs_last(x, y, tw[0], tw[1], q, q2);
+                if (sg == 0) Arith::gs_last(x, y, f0, f1, q, q2);
                 else {
                     const TwPair w = tw[(1u << sg) + j];
                     Arith::gs(x, y, w.w, w.wp, q, q2);
@@ -50,8 +59,14 @@ __global__ void small_kernel(SmallArgs p) {
     uint32_t* a = p.data + (size_t)poly * p.poly_stride + ((size_t)limb << p.logN);
     const TwPair* tw = p.tw + ((size_t)limb << p.logN);
     const uint32_t q = p.q[limb];
-    if (q < (1u << 30)) small_body<Lazy4, Fwd>(a, tw, q, p.logN, s);
-    else small_body<Lazy2, Fwd>(a, tw, q, p.logN, s);
+    TwPair f0 = tw[0], f1 = tw[1];
+    if (p.scale) {
+        const uint32_t c = p.scale[limb] % q;
+        f0 = small_scaled(f0, c, q);
+        f1 = small_scaled(f1, c, q);
+    }
+    if (q < (1u << 30)) small_body<Lazy4, Fwd>(a, tw, q, p.logN, s, f0, f1);
+    else small_body<Lazy2, Fwd>(a, tw, q, p.logN, s, f0, f1);
 }
 
 cudaError_t launch_small(const SmallArgs& a, bool fwd, cudaStream_t s) {

@@ -13,6 +13,7 @@ struct SmallArgs {
     uint32_t jobs;
     unsigned long long poly_stride;
     int logN;
+    const uint32_t* scale;  // optional per-limb constant folded into stage 0
 };
 cudaError_t launch_small(const SmallArgs& a, bool fwd, cudaStream_t s);
 }  // namespace nttb

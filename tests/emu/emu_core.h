@@ -233,6 +233,7 @@ struct EmuCtx {
         }
         return twp[i];
     }
+    TwPair fold_at(uint32_t i) { return tw_at(i); }
     uint32_t tw_base(uint32_t i) { return i; }
     TwPair tw_ld(uint32_t b, uint32_t c) { return tw_at(b + c); }
     void tw_ld2(uint32_t b, uint32_t c, TwPair& x, TwPair& y) {
