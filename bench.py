@@ -337,6 +337,17 @@ def run_ours(args):
     if not torch.equal(host_out, host_in):
         raise RuntimeError("e2e roundtrip is not the identity")
 
+    # the plain per-call form of the same workload: one forward and one
+    # inverse call per polynomial (the reference driver's usage pattern)
+    views = [d[p * LIMBS * N:(p + 1) * LIMBS * N] for p in range(P)]
+
+    def per_call_step():
+        for v in views:
+            plan.forward(v, sh)
+            plan.inverse(v, sh)
+    per_call_ms = device_time(torch, stream, per_call_step, max(3, K // 100), 3)
+    per_call_ms = max_over_ranks(per_call_ms)
+
     transforms = 2 * P * LIMBS * K * world
     value = transforms / (elapsed_max / 1000.0)
     e2e_value = 2 * P * LIMBS * E * world / (e2e_ms / 1000.0)
@@ -383,6 +394,9 @@ def run_ours(args):
                 "pipeline": f"{chunks} chunks of polynomials on 3 streams (host-to-device copy, "
                             "forward + inverse, device-to-host copy)"},
         "gpu_launches": 2 * K,
+        "per_call": {"value": 2 * P * LIMBS * world / (per_call_ms / 1000.0), "unit": "limb-NTT/s",
+                     "ms_per_step": per_call_ms, "launches_per_step": 2 * P,
+                     "form": "one ntt_forward + one ntt_inverse call per polynomial"},
         "roofline": {"bound": "hbm", "kernel": f"fused_kernel ({dom})", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src,
@@ -417,11 +431,41 @@ def run_ours(args):
                                "kind": kind,
                                "sample": f"{reps} forward+inverse roundtrips of one 2^16 x 16 "
                                          f"polynomial in {el:.1f} s"}
+    out["summary"] = summary(out)  # last key: the compact figures survive a cut stdout tail
     if rank == 0:
         print(json.dumps(out))
     plan.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def summary(out):
+    """The headline figures of every leg in a few hundred bytes."""
+    r = lambda v, n=3: None if v is None else round(float(v), n)
+    s = {"value": r(out["value"], 1), "e2e": r(out["e2e"]["value"], 1),
+         "roofline_frac": r(out["roofline"]["frac"]),
+         "forward_ms": r(out["roofline"]["forward_ms"], 4),
+         "inverse_ms": r(out["roofline"]["inverse_ms"], 4)}
+    if "per_call" in out:
+        s["per_call_value"] = r(out["per_call"]["value"], 1)
+    if "batched" in out:
+        s["batched_value"] = r(out["batched"]["value"], 1)
+        s["batched_speedup_vs_plain"] = r(out["batched"]["speedup_vs_plain"])
+    if "fused_multiply" in out:
+        fm = out["fused_multiply"]
+        s["multiply_speedup_vs_unfused"] = r(fm["speedup_vs_unfused"])
+        s["multiply_plan_speedup_vs_unfused"] = r(fm["plan_fused"]["speedup_vs_unfused"])
+    if "serve" in out:
+        for leg in ("host", "device"):
+            L = out["serve"][leg]
+            b, p = L["batched"], L["per_call"]
+            s[f"serve_{leg}_capacity_ratio"] = r(L["capacity_speedup_vs_per_call"])
+            s[f"serve_{leg}_batched_rps"] = r(b["capacity"]["achieved_rps"], 1)
+            s[f"serve_{leg}_p99_ms"] = [r(x["p99_ms"]) for x in b["poisson"]]
+            s[f"serve_{leg}_per_call_p99_ms_at_half"] = r(p["poisson"][0]["p99_ms"])
+    if "cpu_baseline" in out:
+        s["cpu_baseline"] = r(out["cpu_baseline"]["value"], 1)
+    return s
 
 
 RAGGED = dict(seed=SEED, count=256, logn=tuple(range(12, 17)), limbs=(1, 48), bits=(30,))
@@ -586,85 +630,111 @@ SERVE = dict(seed=SEED, logn=tuple(range(12, 18)), limbs=(1, 64), bits=(30, 31),
 
 def bench_serve(args, torch, nb):
     """Serving stream: requests with logN uniform in 12..17, limbs uniform in
-    1..64, 30/31-bit moduli chains, 40% NTT / 40% INTT / 20% multiply, host
-    (pinned) buffers in and out.  Capacity = all requests submitted at once;
-    then Poisson arrivals at fractions of that capacity (open loop), p50/p99
-    of submit -> result-in-host-buffer.  The plain per-call form is the same
-    server with batching off (one request per launch, one stream)."""
+    1..64, 30/31-bit moduli chains, 40% NTT / 40% INTT / 20% multiply.
+    Two legs: host buffers (pinned; each request's polynomial crosses PCIe
+    both ways) and device-resident buffers (each request transformed where
+    it lies in HBM: the GPU is the bound).  In each leg the batched server
+    (rounds of up to 1024 tiles, 4 rounds in flight) is compared with the
+    plain per-call form: the same server with one request per launch and
+    the same 4 stream slots, so the ratio isolates batching.  Capacity = all
+    requests submitted at once; then Poisson arrivals at fractions of that
+    capacity (open loop), p50/p99 of submit -> result (in the host buffer,
+    or on the device)."""
     from ntt_b200 import mixes
     jobs = mixes.ragged_mix(count=args.serve_requests, **SERVE)
-    # preload every modulus the stream names (tables stay resident)
     for lg in SERVE["logn"]:
         for b in SERVE["bits"]:
             nb.tables_preload(lg, mixes.prime_pool(lg, b, 96))
-    # host pools: inputs < 2^29 are valid for every op and modulus; outputs of
-    # the same logN share one pinned buffer (their contents are not checked)
     gen = torch.Generator().manual_seed(SEED)
-    pool = {lg: torch.randint(0, 1 << 29, (64, 1 << lg), dtype=torch.int32, generator=gen)
-                 .pin_memory().numpy().view(np.uint32) for lg in SERVE["logn"]}
-    sink = {lg: torch.empty((64, 1 << lg), dtype=torch.int32).pin_memory().numpy()
-                 .view(np.uint32) for lg in SERVE["logn"]}
     limb_ntts = sum(j.limbs * (3 if j.op == nb.OP_MULTIPLY else 1) for j in jobs)
-    byts = sum(j.words * 4 * (3 if j.op == nb.OP_MULTIPLY else 2) for j in jobs)
+    pcie = sum(j.words * 4 * (3 if j.op == nb.OP_MULTIPLY else 2) for j in jobs)
+    # host leg: inputs < 2^29 are valid for every op and modulus; outputs of
+    # the same logN share one pinned buffer (their contents are not checked)
+    hpool = {lg: torch.randint(0, 1 << 29, (64, 1 << lg), dtype=torch.int32, generator=gen)
+                  .pin_memory().numpy().view(np.uint32) for lg in SERVE["logn"]}
+    hsink = {lg: torch.empty((64, 1 << lg), dtype=torch.int32).pin_memory().numpy()
+                  .view(np.uint32) for lg in SERVE["logn"]}
+    # device leg: requests run in place on a ring of device slots per logN;
+    # multiply operands come from a read-only device pool
+    RING = 32
+    dpool = {lg: torch.randint(0, 1 << 29, (64, 1 << lg), dtype=torch.int32, device="cuda")
+             for lg in SERVE["logn"]}
+    dring = {lg: torch.randint(0, 1 << 29, (RING, 64, 1 << lg), dtype=torch.int32,
+                               device="cuda") for lg in SERVE["logn"]}
 
-    def run(srv, rate):
+    def prepare(srv, device):
+        out, k = [], {lg: 0 for lg in SERVE["logn"]}
+        for j in jobs:
+            if device:
+                slot = dring[j.logN][k[j.logN] % RING][:j.limbs]
+                k[j.logN] += 1
+                x = o = slot
+                a = dpool[j.logN][:j.limbs] if j.op == nb.OP_MULTIPLY else None
+            else:
+                x, o = hpool[j.logN][:j.limbs], hsink[j.logN][:j.limbs]
+                a = x if j.op == nb.OP_MULTIPLY else None
+            out.append(srv.request(j.op, j.logN, j.moduli, x, o, operand=a, device=device))
+        return out
+
+    def run(srv, reqs, rate):
         srv.stats(reset=True)
         rng = np.random.default_rng(SEED)
-        gaps = rng.exponential(1.0 / rate, len(jobs)) if rate else None
-        t0 = time.perf_counter()
-        t_next = t0
+        gaps = rng.exponential(1.0 / rate, len(reqs)) if rate else None
+        t_next = time.perf_counter()
         tickets = []
-        for i, j in enumerate(jobs):
+        for i, r in enumerate(reqs):
             if gaps is not None:
                 t_next += gaps[i]
-                while time.perf_counter() < t_next:
-                    pass
-            x = pool[j.logN][:j.limbs]
-            tickets.append(srv.submit(j.op, j.logN, j.moduli, x, sink[j.logN][:j.limbs],
-                                      operand=x if j.op == nb.OP_MULTIPLY else None))
+                while True:
+                    dt = t_next - time.perf_counter()
+                    if dt <= 0:
+                        break
+                    if dt > 2e-4:
+                        time.sleep(dt - 1e-4)
+            tickets.append(srv.submit_prepared(r))
         for t in tickets:
             srv.wait(t, 300.0)
         st = srv.stats(reset=True)
-        return {"offered_rps": rate, "achieved_rps": len(jobs) / st["elapsed_s"],
+        return {"offered_rps": rate, "achieved_rps": len(reqs) / st["elapsed_s"],
                 "limb_ntt_per_s": st["limb_ntt_per_s"], "p50_ms": st["p50_ms"],
                 "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
                 "rounds": st["rounds"], "mean_round_requests": st["mean_round_requests"],
                 "arena_peak_bytes": st["arena_peak_bytes"], "elapsed_s": st["elapsed_s"]}
 
-    loads = [float(v) for v in args.serve_loads.split(",") if v]
-    out = {"workload": f"{len(jobs)} requests: logN uniform 12..17, limbs uniform 1..64, 30/31-bit "
-                       "chains, 40% NTT / 40% INTT / 20% multiply, pinned host buffers in and "
-                       "out; latency = submit -> result in the host buffer",
-           "limb_ntts": limb_ntts, "pcie_bytes": byts}
-    with nb.Server() as srv:  # 80 GB budget, 4 streams, rounds of up to 1024 tiles
-        # correctness spot check against the plain per-call path
-        chk = [j for j in jobs[:200] if j.limbs <= 8][:6]
-        for j in chk:
-            x = pool[j.logN][:j.limbs].copy()
+    def form(device, batched, loads):
+        kw = {} if batched else {"max_round_requests": 1}
+        with nb.Server(streams=4, **kw) as srv:
+            reqs = prepare(srv, device)
+            cap = run(srv, reqs, None)
+            res = {"capacity": cap,
+                   "poisson": [run(srv, reqs, f * cap["achieved_rps"]) for f in loads]}
+            res["budget_bytes"] = srv.stats()["budget_bytes"]
+        return res
+
+    # correctness spot check of the served path against the plain path
+    with nb.Server() as srv:
+        for j in [j for j in jobs[:200] if j.limbs <= 8 and j.op != nb.OP_MULTIPLY][:6]:
+            x = hpool[j.logN][:j.limbs].copy()
             o = np.empty_like(x)
-            srv.wait(srv.submit(j.op, j.logN, j.moduli, x, o,
-                                operand=x if j.op == nb.OP_MULTIPLY else None), 60.0)
+            srv.wait(srv.submit(j.op, j.logN, j.moduli, x, o), 60.0)
             p = nb.Plan(j.logN, j.moduli)
             d = torch.from_numpy(x.view(np.int32)).cuda()
-            if j.op == nb.OP_FORWARD:
-                p.forward(d)
-            elif j.op == nb.OP_INVERSE:
-                p.inverse(d)
-            else:
-                continue  # multiply parity is covered by the tests
+            (p.forward if j.op == nb.OP_FORWARD else p.inverse)(d)
             torch.cuda.synchronize()
             if not np.array_equal(d.cpu().numpy().view(np.uint32), o):
                 raise RuntimeError("served result differs from the plain path")
             p.close()
-        cap = run(srv, None)
-        out["batched"] = {"capacity": cap, "poisson": [run(srv, f * cap["achieved_rps"])
-                                                         for f in loads]}
-        out["budget_bytes"] = srv.stats()["budget_bytes"]
-    with nb.Server(streams=1, max_round_requests=1) as srv:
-        cap_p = run(srv, None)
-        out["plain_per_call"] = {"capacity": cap_p,
-                                 "poisson": [run(srv, 0.5 * cap_p["achieved_rps"])]}
-    out["capacity_speedup_vs_plain"] = cap["achieved_rps"] / cap_p["achieved_rps"]
+    loads = [float(v) for v in args.serve_loads.split(",") if v]
+    out = {"workload": f"{len(jobs)} requests: logN uniform 12..17, limbs uniform 1..64, "
+                       "30/31-bit chains, 40% NTT / 40% INTT / 20% multiply",
+           "limb_ntts": limb_ntts, "pcie_bytes_host_leg": pcie,
+           "per_call_form": "the same server, one request per launch, same 4 stream slots"}
+    for leg, device in (("host", False), ("device", True)):
+        b = form(device, True, loads)
+        p = form(device, False, [0.5])
+        out[leg] = {"batched": b, "per_call": p,
+                    "capacity_speedup_vs_per_call":
+                        b["capacity"]["achieved_rps"] / p["capacity"]["achieved_rps"]}
     return out
 
 

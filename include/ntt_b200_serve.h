@@ -12,6 +12,9 @@
  * are admitted as soon as a stream and arena space are free, and their
  * copies and transforms overlap the running ones on the device.
  *
+ * Requests may instead name device-resident buffers (device_buffers): they
+ * are transformed where they lie, so only the device's own work counts.
+ *
  * Memory: the arena (`hbm_budget_bytes`, reserved at creation) holds the
  * polynomials of admitted requests and the resident operands; a request
  * waits in FIFO order until its bytes fit.  Twiddle tables live in the
@@ -49,6 +52,11 @@ typedef struct ntt_request {
                                      _MULTIPLY_SPECTRUM (or use operand_handle) */
     uint64_t operand_handle;      /* resident operand from ntt_server_put (0 = none) */
     uint32_t* output;             /* host, limbs * 2^logN words (may equal input) */
+    int device_buffers;           /* nonzero: input, operand and output are device
+                                     buffers on the server's device (16-byte aligned);
+                                     the request runs on `output` in place (after a
+                                     device copy of `input` when they differ), takes no
+                                     arena space and moves nothing over PCIe */
 } ntt_request_t;
 
 typedef struct ntt_server_stats {

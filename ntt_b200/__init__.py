@@ -569,7 +569,8 @@ def tables_preload(logN: int, moduli: Sequence):
 class Request(ctypes.Structure):
     _fields_ = [("op", ctypes.c_int), ("logN", ctypes.c_int), ("limbs", ctypes.c_int),
                 ("moduli", ctypes.POINTER(ModulusConfig)), ("input", _vp), ("operand", _vp),
-                ("operand_handle", ctypes.c_uint64), ("output", _vp)]
+                ("operand_handle", ctypes.c_uint64), ("output", _vp),
+                ("device_buffers", ctypes.c_int)]
 
 
 class ServerOptions(ctypes.Structure):
@@ -636,17 +637,30 @@ class Server:
         self._h = h
         self._live = {}
 
-    def submit(self, op: int, logN: int, moduli: Sequence, input, output, operand=None,
-               operand_handle: int = 0) -> int:
+    def request(self, op: int, logN: int, moduli: Sequence, input, output, operand=None,
+                operand_handle: int = 0, device: bool = False):
+        """A prepared request (for submit_prepared): device=True takes device
+        tensors that are transformed in place (input copied into output
+        first when they differ)."""
         m, n = _moduli_array(moduli)
-        r = Request(op, logN, n, ctypes.cast(m, ctypes.POINTER(ModulusConfig)), _host_ptr(input),
-                    _host_ptr(operand) if operand is not None else None, operand_handle,
-                    _host_ptr(output))
+        p = _ptr if device else _host_ptr
+        r = Request(op, logN, n, ctypes.cast(m, ctypes.POINTER(ModulusConfig)), p(input),
+                    p(operand) if operand is not None else None, operand_handle, p(output),
+                    1 if device else 0)
+        return r, (m, input, output, operand)
+
+    def submit_prepared(self, prepared) -> int:
+        r, keep = prepared
         t = ctypes.c_uint64()
         _check(_lib.ntt_server_submit(self._h, ctypes.byref(r), ctypes.byref(t)),
                "ntt_server_submit")
-        self._live[t.value] = (input, output, operand)
+        self._live[t.value] = keep
         return t.value
+
+    def submit(self, op: int, logN: int, moduli: Sequence, input, output, operand=None,
+               operand_handle: int = 0, device: bool = False) -> int:
+        return self.submit_prepared(self.request(op, logN, moduli, input, output, operand,
+                                                 operand_handle, device))
 
     def poll(self, ticket: int) -> bool:
         st = _lib.ntt_server_poll(self._h, ticket)

@@ -80,6 +80,7 @@ struct Req {
     const uint32_t* operand = nullptr;
     uint64_t operand_handle = 0;
     uint32_t* output = nullptr;
+    bool dev = false;                       // device-resident buffers (no arena, no PCIe)
     size_t bytes = 0;                       // one polynomial
     size_t off_data = kNone, off_op = kNone;  // arena slots owned by the request
     size_t res_off = kNone;                     // resident operand (owned by its handle)
@@ -87,6 +88,7 @@ struct Req {
     Clock::time_point t_submit, t_done;
     ntt_status_t status = NTT_ERR_NOT_READY;
     size_t arena_need() const {
+        if (dev) return 0;
         return bytes + (batch_op_is_multiply((uint32_t)op) && !operand_handle ? bytes : 0);
     }
 };
@@ -172,12 +174,20 @@ ntt_status_t issue_round(ntt_server* S, Slot& sl) {
     std::vector<BatchTile> tiles;
     int max_logn = 0;
     for (auto& r : sl.reqs) {
-        char* data = S->arena_base + r->off_data;
-        if (cudaMemcpyAsync(data, r->input, r->bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        char* data = r->dev ? (char*)r->output : S->arena_base + r->off_data;
+        if (r->dev) {
+            if (r->input != r->output &&
+                cudaMemcpyAsync(data, r->input, r->bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+                return cuda_fail(cudaGetLastError(), "round input copy (device)");
+        } else if (cudaMemcpyAsync(data, r->input, r->bytes, cudaMemcpyHostToDevice, s) !=
+                   cudaSuccess) {
             return cuda_fail(cudaGetLastError(), "round input copy");
+        }
         const uint32_t* opnd = nullptr;
         if (batch_op_is_multiply((uint32_t)r->op)) {
-            if (r->operand_handle) {
+            if (r->dev && !r->operand_handle) {
+                opnd = r->operand;
+            } else if (r->operand_handle) {
                 opnd = (const uint32_t*)(S->arena_base + r->res_off);
             } else {
                 if (cudaMemcpyAsync(S->arena_base + r->off_op, r->operand, r->bytes,
@@ -229,8 +239,8 @@ ntt_status_t issue_round(ntt_server* S, Slot& sl) {
     if (ntt_status_t st = batch_launch(a, v, std::min<int>(resident, (int)rounds.size()), s))
         return st;
     for (auto& r : sl.reqs)
-        if (cudaMemcpyAsync(r->output, S->arena_base + r->off_data, r->bytes,
-                            cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        if (!r->dev && cudaMemcpyAsync(r->output, S->arena_base + r->off_data, r->bytes,
+                                       cudaMemcpyDeviceToHost, s) != cudaSuccess)
             return cuda_fail(cudaGetLastError(), "round output copy");
     if (cudaEventRecord(sl.done, s) != cudaSuccess)
         return cuda_fail(cudaGetLastError(), "round event");
@@ -273,6 +283,23 @@ void scheduler_main(ntt_server* S) {
             if (!take.empty() && tiles + (size_t)r->limbs > (size_t)S->opt.max_round_tiles) break;
             if (S->opt.max_round_requests && take.size() >= (size_t)S->opt.max_round_requests)
                 break;
+            if (r->dev) {  // runs where it lies: no arena space
+                if (r->operand_handle) {
+                    auto it = S->resident.find(r->operand_handle);
+                    if (it == S->resident.end() || it->second.second < r->bytes) {
+                        S->pending.pop_front();
+                        r->status = fail(NTT_ERR_INVALID_ARGUMENT, "unknown or short operand handle");
+                        ++S->failed;
+                        S->cv_done.notify_all();
+                        continue;
+                    }
+                    r->res_off = it->second.first;
+                }
+                take.push_back(r);
+                tiles += (size_t)r->limbs;
+                S->pending.pop_front();
+                continue;
+            }
             const size_t od = S->arena.alloc(r->bytes);
             if (od == kNone) break;
             size_t oo = kNone;
@@ -376,7 +403,11 @@ ntt_status_t ntt_server_create(const ntt_server_options_t* opts, ntt_server_t** 
         auto sl = std::make_unique<Slot>();
         sl->desc_bytes = desc;
         cudaError_t e = cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming);
+        // completion threads sleep in cudaEventSynchronize instead of
+        // spinning: on a shared host, four spinning threads next to the
+        // caller's submit loop showed up as multi-millisecond latency tails
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming | cudaEventBlockingSync);
         if (e == cudaSuccess) e = cudaMalloc(&sl->dev_desc, desc);
         if (e == cudaSuccess) e = cudaHostAlloc(&sl->host_desc, desc, cudaHostAllocDefault);
         S->slots.push_back(std::move(sl));
@@ -409,6 +440,9 @@ ntt_status_t ntt_server_submit(ntt_server_t* S, const ntt_request_t* q, uint64_t
         return fail(NTT_ERR_UNSUPPORTED, "more limbs than a round holds (%d)", S->opt.max_round_tiles);
     if (batch_op_is_multiply((uint32_t)q->op) && !q->operand && !q->operand_handle)
         return fail(NTT_ERR_INVALID_ARGUMENT, "multiply needs an operand");
+    if (q->device_buffers &&
+        (((uintptr_t)q->input | (uintptr_t)q->output | (uintptr_t)q->operand) & 15u) != 0)
+        return fail(NTT_ERR_MISALIGNED, "device buffers must be 16-byte aligned");
     auto r = std::make_shared<Req>();
     r->op = q->op;
     r->logN = q->logN;
@@ -417,6 +451,7 @@ ntt_status_t ntt_server_submit(ntt_server_t* S, const ntt_request_t* q, uint64_t
     r->operand = q->operand;
     r->operand_handle = batch_op_is_multiply((uint32_t)q->op) ? q->operand_handle : 0;
     r->output = q->output;
+    r->dev = q->device_buffers != 0;
     r->bytes = ((size_t)q->limbs << q->logN) * 4;
     if (r->arena_need() > S->arena_size)
         return fail(NTT_ERR_BUDGET, "request needs %zu bytes, arena holds %zu", r->arena_need(),

@@ -215,3 +215,47 @@ def test_in_place_output_and_errors(torch_cuda, nb, mixes):
         with pytest.raises(nb.NttError) as e:
             srv.wait(123456, 0.1)
         assert e.value.name == "NTT_ERR_INVALID_ARGUMENT"
+
+
+def test_device_resident_requests_match_plain(torch_cuda, nb, mixes):
+    """Requests on device buffers (device_buffers): transformed where they
+    lie, in place or from a distinct input, mixed in one stream with
+    host-buffer requests; every result equals the plain per-call path."""
+    torch = torch_cuda
+    jobs = mixes.ragged_mix(seed=35, count=60, logn=range(12, 18), limbs=(1, 6), bits=(30, 31),
+                            ops=((nb.OP_FORWARD, 2), (nb.OP_INVERSE, 2), (nb.OP_MULTIPLY, 1)))
+    rng = np.random.default_rng(5)
+    ins = [rand_poly(rng, j) for j in jobs]
+    opnds = [rand_poly(rng, j) if j.op == nb.OP_MULTIPLY else None for j in jobs]
+    dev = lambda a: torch.from_numpy(a.view(np.int32)).cuda()
+    outs, keep = [], []
+    with nb.Server(hbm_budget_bytes=1 << 30) as srv:
+        tickets = []
+        for i, j in enumerate(jobs):
+            if i % 3 == 2:  # host buffers
+                o = np.empty_like(ins[i])
+                tickets.append(srv.submit(j.op, j.logN, j.moduli, ins[i], o, operand=opnds[i]))
+            else:
+                x = dev(ins[i])
+                o = x if i % 3 == 0 else torch.empty_like(x)  # in place / distinct output
+                a = dev(opnds[i]) if opnds[i] is not None else None
+                keep.append((x, a))
+                tickets.append(srv.submit(j.op, j.logN, j.moduli, x, o, operand=a, device=True))
+            outs.append(o)
+        for t in tickets:
+            srv.wait(t, 60.0)
+        st = srv.stats()
+    assert st["completed"] == len(jobs) and st["failed"] == 0
+    for i, j in enumerate(jobs):
+        got = outs[i] if isinstance(outs[i], np.ndarray) else outs[i].cpu().numpy().view(np.uint32)
+        assert np.array_equal(got, plain(torch, nb, j, ins[i], opnds[i])), f"request {i}"
+
+
+def test_device_buffers_must_be_aligned(torch_cuda, nb, mixes):
+    torch = torch_cuda
+    pool = mixes.prime_pool(12, 30, 2)
+    x = torch.zeros(2 * (1 << 12) + 4, dtype=torch.int32, device="cuda")
+    with nb.Server(hbm_budget_bytes=1 << 28) as srv:
+        with pytest.raises(nb.NttError) as e:
+            srv.submit(nb.OP_FORWARD, 12, pool, x[1:], x[1:], device=True)
+        assert e.value.name == "NTT_ERR_MISALIGNED"
