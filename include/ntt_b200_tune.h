@@ -29,6 +29,11 @@ typedef struct ntt_kernel_config {
     int polys_per_job;   /* polynomials whose same limb one cluster
                             transforms together, sharing every twiddle
                             load (1, or 2 for the paired configurations) */
+    int exchange;        /* how the limb's two phases meet: 0 = scatter into
+                            the peers' shared memory (DSMEM), 1 = in place
+                            through L2 (split kernels: phase 1 is one register
+                            pass per column, phase 2 two or three passes)     */
+    int k2b;             /* split kernels: stages of the second phase-2 pass */
 } ntt_kernel_config_t;
 
 typedef struct ntt_tune_result {

@@ -87,7 +87,8 @@ class KernelConfig(ctypes.Structure):
     _fields_ = [("logN", ctypes.c_int), ("cluster_ctas", ctypes.c_int), ("r1", ctypes.c_int),
                 ("words_log2", ctypes.c_int), ("k1a", ctypes.c_int), ("k2a", ctypes.c_int),
                 ("threads", ctypes.c_int), ("smem_bytes", ctypes.c_uint32),
-                ("polys_per_job", ctypes.c_int)]
+                ("polys_per_job", ctypes.c_int), ("exchange", ctypes.c_int),
+                ("k2b", ctypes.c_int)]
 
 
 class TuneResult(ctypes.Structure):

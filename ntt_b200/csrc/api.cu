@@ -106,6 +106,18 @@ const FusedConfig* default_single_config(int logN, bool fwd) {
     return d;
 }
 
+// The untuned cluster (scatter) configuration for logN with `np` polynomials
+// per job (the forward default's pick when it is one), for launches that need
+// the product epilogue.
+const FusedConfig* cluster_config(int logN, int np) {
+    const FusedConfig* c = fused_configs();
+    for (const FusedConfig* d : {default_config(logN, true), default_single_config(logN, true)})
+        if (d && !d->split && d->np == np) return d;
+    for (int i = 0; i < fused_config_count(); ++i)
+        if (c[i].logN == logN && !c[i].split && c[i].np == np) return &c[i];
+    return nullptr;
+}
+
 const FusedConfig* config_by_r1(int logN, int r1) {
     const FusedConfig* c = fused_configs();
     for (int i = 0; i < fused_config_count(); ++i)
@@ -128,6 +140,14 @@ void effective_triples(const FusedConfig* c, int logN, TransformConfig* t) {
         return;
     }
     const int r2 = logN - c->r1;
+    if (c->split) {  // one phase-1 pass per column; phase 2 in two or three passes
+        const int k2c = r2 - c->k2a - c->k2b;
+        int m2 = c->k2a > c->k2b ? c->k2a : c->k2b;
+        if (k2c > m2) m2 = k2c;
+        const PhaseConfig p1{c->r1, c->r1, 0}, p2{r2, m2, c->eb};
+        *t = TransformConfig{p1, p2, p2, p1};
+        return;
+    }
     const int k1b = c->r1 - c->k1a, k2b = r2 - c->k2a;
     const int s1 = r2 - c->clog;
     int run1 = c->eb - c->k1a;
@@ -615,6 +635,11 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
     if (!a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL data pointer");
     if (mul_src && (!cfg || !fwd))
         return fail(NTT_ERR_UNSUPPORTED, "the product epilogue needs a fused forward (logN >= 10)");
+    // split configurations transform in place through the data buffer, which
+    // the product epilogue needs intact: it runs on a cluster configuration
+    if (mul_src && cfg && !cfg->has_mul()) cfg = cluster_config(logN, cfg->np);
+    if (mul_src && !cfg)
+        return fail(NTT_ERR_UNSUPPORTED, "no configuration with the product epilogue for logN %d", logN);
     if (mul_src && (((uintptr_t)mul_src & 15u) != 0))
         return fail(NTT_ERR_MISALIGNED, "data must be 16-byte aligned (stride a multiple of 4 words)");
     // the fused kernels move 16-byte vectors; the small-size kernel words

@@ -34,6 +34,15 @@
     NTTB_CFG_N10(X) NTTB_CFG_N11(X) NTTB_CFG_N12(X) NTTB_CFG_N13(X) NTTB_CFG_N14(X)      \
     NTTB_CFG_N15(X) NTTB_CFG_N16(X) NTTB_CFG_N16B(X) NTTB_CFG_N16M(X) NTTB_CFG_N17(X)
 
+// Split configurations (split_kernel.cuh): S(LOGN, CLOG, EB, K2A, K2B).
+//   Phase 1 = EB row stages, one register pass per column straight from and
+//   back to global memory; the limb's CTAs then exchange through L2 (in
+//   place) across one cluster barrier; phase 2 = passes of K2A, K2B and
+//   LOGN - EB - K2A - K2B (if nonzero) stages over the CTA's contiguous rows.
+#define NTTB_SPLIT_N16(S) S(16, 3, 5, 4, 4) S(16, 3, 4, 4, 4)
+#define NTTB_SPLIT_REST(S) S(17, 4, 5, 4, 4) S(15, 2, 5, 5, 5) S(15, 2, 4, 4, 4)
+#define NTTB_SPLIT_ALL(S) NTTB_SPLIT_N16(S) NTTB_SPLIT_REST(S)
+
 #include <cstdint>
 
 namespace nttb {
@@ -48,7 +57,11 @@ struct FusedConfig {
     // direct kernels (run over resident chunks of jobs)
     const void* kern[2][2][2];
     // the direct forward with the product epilogue (fused_kernel<..., Mul>): [lazy2]
+    // (nullptr for split configurations: a cluster configuration runs it)
     const void* kern_mul[2];
+    int split;  // 1: split configuration (exchange through L2), 0: cluster scatter
+    int k2b;    // split: stages of the second phase-2 pass
+    bool has_mul() const { return kern_mul[0] != nullptr; }
     const void* kernel(bool staged, bool fwd, bool lazy2) const {
         return kern[staged ? 1 : 0][fwd ? 1 : 0][lazy2 ? 1 : 0];
     }

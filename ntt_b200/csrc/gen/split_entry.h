@@ -1,0 +1,18 @@
+// FusedConfig table entry of split configuration S(N, CL, EB, K2A, K2B)
+// (configs.h, split_kernel.cuh): the kernel loops over its cluster's jobs, so
+// the direct and the staged schedule run the same kernel; the forward with
+// the product epilogue is left to a cluster configuration (kern_mul null).
+#pragma once
+#include "../configs.h"
+#include "../split_kernel.cuh"
+
+#define NTTB_SG(N, CL, EB, KA, KB) SplitGeo<N, CL, EB, KA, KB>
+#define NTTB_SK(N, CL, EB, KA, KB, F, A) (const void*)&split_kernel<NTTB_SG(N, CL, EB, KA, KB), F, A>
+#define NTTB_SPLIT_ENTRY(N, CL, EB, KA, KB)                                                     \
+    {N, CL, EB, EB, EB, KA, 1, NTTB_SG(N, CL, EB, KA, KB)::THREADS,                              \
+     NTTB_SG(N, CL, EB, KA, KB)::SMEM_BYTES, NTTB_SG(N, CL, EB, KA, KB)::SMEM_BYTES,            \
+     {{{NTTB_SK(N, CL, EB, KA, KB, false, Lazy4), NTTB_SK(N, CL, EB, KA, KB, false, Lazy2)},     \
+       {NTTB_SK(N, CL, EB, KA, KB, true, Lazy4), NTTB_SK(N, CL, EB, KA, KB, true, Lazy2)}},      \
+      {{NTTB_SK(N, CL, EB, KA, KB, false, Lazy4), NTTB_SK(N, CL, EB, KA, KB, false, Lazy2)},     \
+       {NTTB_SK(N, CL, EB, KA, KB, true, Lazy4), NTTB_SK(N, CL, EB, KA, KB, true, Lazy2)}}},     \
+     {nullptr, nullptr}, 1, KB},

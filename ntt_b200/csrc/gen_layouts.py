@@ -226,6 +226,68 @@ def mask(pos):
     return sum(1 << p for p in pos)
 
 
+# ---------------------------------------------------------------------------
+# Split (L2-exchange) configurations: phase 1 is one register pass per column
+# in global memory (no shared memory); phase 2 runs two or three register
+# passes over the CTA's contiguous rows in the work buffer.  The first phase-2
+# pass reads global memory with its lanes on the 5 lowest bits (its extra
+# register bits are the lowest free positions from bit 5 up); the others
+# follow PassLayout's rule.  Mirrors SplitGeo in split_kernel.cuh.
+# ---------------------------------------------------------------------------
+
+def split_configs():
+    src = open(os.path.join(HERE, "configs.h")).read()
+    src = src.split("// Split configurations")[1].split("#include")[0]
+    out = []
+    for m in re.findall(r"S\((\d+), (\d+), (\d+), (\d+), (\d+)\)", src):
+        g = tuple(int(v) for v in m)
+        if g not in out:
+            out.append(g)
+    return out
+
+
+def split_passes(N, CL, EB, K2A, K2B):
+    MB, R2 = N - CL, N - EB
+    K2C = R2 - K2A - K2B
+    lo_a, lo_b = R2 - K2A, R2 - K2A - K2B
+    # first pass: explicit extras from bit 5 up
+    extra = [p for p in range(5, MB) if not (lo_a <= p < lo_a + K2A)][:EB - K2A]
+    reg_a = set(range(lo_a, lo_a + K2A)) | set(extra)
+    lanes_a = [p for p in range(MB) if p not in reg_a][:5]
+    out = [("P2A", lanes_a, run_bits(reg_a), False)]
+    out.append(("P2B", pass_lanes(MB, lo_b, K2B, EB, 0), run_bits(pass_regs(MB, lo_b, K2B, EB, 0)), True))
+    if K2C > 0:
+        out.append(("P2C", pass_lanes(MB, 0, K2C, EB, 0), run_bits(pass_regs(MB, 0, K2C, EB, 0)), True))
+    return MB, out
+
+
+def split_layout(cfg):
+    N, CL, EB, K2A, K2B = cfg
+    MB, ps = split_passes(*cfg)
+    E = 1 << EB
+    best = None
+    cs = [1, 2, 3, 4, 5, 6, 7, 8, 12, 16, 20, 24, 28, 32, 36, 40]
+    top = (1 << MB) - 1
+    cands = [(a1, c1, MB, 0) for a1 in range(MB) for c1 in cs]
+    cands += [(a1, c1, a2, c2) for a1 in range(MB) for c1 in cs
+              for a2 in range(a1 + 1, MB) for c2 in cs]
+    for lay in cands:
+        if phys(top, *lay) + 1 > (top + 1) * 9 // 8:
+            continue
+        worst, cost = 1, 0
+        for name, pos, run, both in ps:  # the first pass only stores
+            d, c = pattern_cost(pos, run, E, lay)
+            worst, cost = max(worst, d), cost + (2 if both else 1) * c
+        chunk = ([2, 3, 4, 5, 6], 2) if aligned(lay, 4) else ([0, 1, 2, 3, 4], 0)
+        d, c = pattern_cost(chunk[0], chunk[1], E, lay)
+        worst, cost = max(worst, d), cost + 2 * c
+        key = (worst, cost, phys(top, *lay) + 1)
+        if best is None or key < best[0]:
+            best = (key, lay)
+    (deg, cost, size), lay = best
+    return lay, size, ps
+
+
 def main():
     lines = [
         "// GENERATED by gen_layouts.py from configs.h -- do not edit.",
@@ -249,6 +311,16 @@ def main():
         lines.append(f"    static constexpr int XW[5] = {{{a1}, {c1}, {a2}, {c2}, {size}}};")
         for name in ("P1A", "P1B", "P2A", "P2B"):
             lines.append(f"    static constexpr uint32_t lanes_{name} = 0x{mask(g[name]):x}u;")
+        lines.append("};")
+        lines.append("")
+    lines += ["template <int N, int CL, int EB, int K2A, int K2B>", "struct SplitLayoutTable;", ""]
+    for cfg in split_configs():
+        (a1, c1, a2, c2), size, ps = split_layout(cfg)
+        lines.append("template <>")
+        lines.append("struct SplitLayoutTable<%d, %d, %d, %d, %d> {" % cfg)
+        lines.append(f"    static constexpr int XW[5] = {{{a1}, {c1}, {a2}, {c2}, {size}}};")
+        for name, pos, run, both in ps:
+            lines.append(f"    static constexpr uint32_t lanes_{name} = 0x{mask(pos):x}u;")
         lines.append("};")
         lines.append("")
     lines.append("}  // namespace nttb")

@@ -208,4 +208,46 @@ struct LayoutTable<17, 4, 6, 6, 6, 5> {
     static constexpr uint32_t lanes_P2B = 0x7c0u;
 };
 
+template <int N, int CL, int EB, int K2A, int K2B>
+struct SplitLayoutTable;
+
+template <>
+struct SplitLayoutTable<16, 3, 5, 4, 4> {
+    static constexpr int XW[5] = {5, 2, 13, 0, 8702};
+    static constexpr uint32_t lanes_P2A = 0x1fu;
+    static constexpr uint32_t lanes_P2B = 0x386u;
+    static constexpr uint32_t lanes_P2C = 0x3e0u;
+};
+
+template <>
+struct SplitLayoutTable<16, 3, 4, 4, 4> {
+    static constexpr int XW[5] = {5, 2, 13, 0, 8702};
+    static constexpr uint32_t lanes_P2A = 0x1fu;
+    static constexpr uint32_t lanes_P2B = 0x10fu;
+    static constexpr uint32_t lanes_P2C = 0x1f0u;
+};
+
+template <>
+struct SplitLayoutTable<17, 4, 5, 4, 4> {
+    static constexpr int XW[5] = {5, 2, 13, 0, 8702};
+    static constexpr uint32_t lanes_P2A = 0x1fu;
+    static constexpr uint32_t lanes_P2B = 0x30eu;
+    static constexpr uint32_t lanes_P2C = 0x3e0u;
+};
+
+template <>
+struct SplitLayoutTable<15, 2, 5, 5, 5> {
+    static constexpr int XW[5] = {5, 4, 13, 0, 9212};
+    static constexpr uint32_t lanes_P2A = 0x1fu;
+    static constexpr uint32_t lanes_P2B = 0x3e0u;
+};
+
+template <>
+struct SplitLayoutTable<15, 2, 4, 4, 4> {
+    static constexpr int XW[5] = {5, 2, 13, 0, 8702};
+    static constexpr uint32_t lanes_P2A = 0x1fu;
+    static constexpr uint32_t lanes_P2B = 0x187u;
+    static constexpr uint32_t lanes_P2C = 0x1f0u;
+};
+
 }  // namespace nttb

@@ -155,6 +155,91 @@ struct PassLayout {
     }
 };
 
+// A register pass whose extra (non-butterfly) register bits are given
+// explicitly (XM) instead of being the lowest free positions; the lane
+// index fills the 5 lowest remaining positions and the warp index the rest.
+// Used where a pass reads global memory and its lanes must cover 32
+// consecutive words (a 128-byte line per warp instruction).
+template <int MB_, int PLO_, int KB_, int EB_, uint32_t XM_>
+struct PassLayoutX {
+    static constexpr int MB = MB_, PLO = PLO_, KB = KB_, EB = EB_;
+    static constexpr int XB = EB - KB;
+    static constexpr int E = 1 << EB;
+    static_assert(KB >= 1 && KB <= EB && EB <= MB && PLO + KB <= MB, "bad pass layout");
+    static_assert(popcount32(XM_) == XB, "one extra mask bit per extra register bit");
+    static constexpr int xpos(int j) {
+        for (int p = 0, c = 0; p < MB; ++p)
+            if ((XM_ >> p) & 1u) {
+                if (c == j) return p;
+                ++c;
+            }
+        return -1;
+    }
+    static constexpr uint32_t reg_mask() {
+        uint32_t m = XM_;
+        for (int p = PLO; p < PLO + KB; ++p) m |= 1u << p;
+        return m;
+    }
+    static constexpr uint32_t off(int r) {
+        uint32_t o = (uint32_t)(r >> XB) << PLO;
+        for (int j = 0; j < XB; ++j)
+            if ((r >> j) & 1) o |= 1u << xpos(j);
+        return o;
+    }
+    static constexpr int reg_of(uint32_t o) {
+        for (int r = 0; r < E; ++r)
+            if (off(r) == o) return r;
+        return -1;
+    }
+    static constexpr int run_bits() {
+        int v = 0;
+        while (v < MB && ((reg_mask() >> v) & 1u)) ++v;
+        return v;
+    }
+    static constexpr int xhi_bits() {
+        int c = 0;
+        for (int j = 0; j < XB; ++j)
+            if (xpos(j) > PLO + KB - 1) ++c;
+        return c;
+    }
+    static constexpr uint32_t kRegMask = reg_mask();
+    static_assert((kRegMask & ~((MB >= 32) ? 0xFFFFFFFFu : ((1u << MB) - 1u))) == 0, "bits");
+    static constexpr int kRunBits = run_bits();
+    static constexpr int kXHB = xhi_bits();
+    static constexpr uint32_t kFull = (MB >= 32) ? 0xFFFFFFFFu : ((1u << MB) - 1u);
+    static constexpr uint32_t lanes() {
+        const uint32_t m = kFull & ~kRegMask;
+        uint32_t out = 0;
+        for (int p = 0, c = 0; p < MB && c < 5; ++p)
+            if ((m >> p) & 1u) {
+                out |= 1u << p;
+                ++c;
+            }
+        return out;
+    }
+    static constexpr uint32_t kLanes = lanes();
+    static constexpr uint32_t WM = kFull & ~kRegMask & ~kLanes;
+    template <uint32_t Mask>
+    NTT_HD static uint32_t deposit(uint32_t x) {
+        uint32_t v = 0;
+        ct_for<MB>([&](auto P) {
+            constexpr int p = decltype(P)::value;
+            if constexpr (((Mask >> p) & 1u) != 0) {
+                constexpr int rank = popcount32(Mask & ((1u << p) - 1u));
+                v |= ((x >> rank) & 1u) << p;
+            }
+        });
+        return v;
+    }
+    NTT_HD static uint32_t dep(uint32_t t) { return deposit<kLanes>(t & 31u) | deposit<WM>(t >> 5); }
+};
+
+// Lambda positions of the warp index of a pass layout (either kind).
+template <class L>
+constexpr uint32_t warp_bits() {
+    return L::kFull & ~L::kRegMask & ~L::kLanes;
+}
+
 // ---------------------------------------------------------------------------
 // Shared-memory layouts.  The work buffer uses one bank-spreading layout
 //     phys(l) = l + C1 * (l >> A1) + C2 * (l >> A2)

@@ -18,6 +18,8 @@ const FusedConfig* default_config(int logN, bool fwd = true);
 // ... for launches of a single polynomial (one polynomial per job).
 const FusedConfig* default_single_config(int logN, bool fwd);
 const FusedConfig* config_by_r1(int logN, int r1);
+// Untuned cluster (scatter) configuration with np polynomials per job.
+const FusedConfig* cluster_config(int logN, int np = 1);
 const FusedConfig* config_by_index(int idx);
 // Autotuned choice for (logN, limbs, direction) on the current device, or
 // nullptr.

@@ -1,0 +1,256 @@
+// Split transform kernels (sm_100a): the limb's two phases exchange through
+// L2 instead of distributed shared memory.
+//
+// Same math and the same twiddle tables as the cluster kernels
+// (fused_kernel.cuh; reference: NTTPhase1/NTTPhase2, INTTPhase1/INTTPhase2,
+// src/v04_montgomery.cu:196-565).  The limb of N = 2^n words is a
+// 2^R1 x 2^R2 matrix, R1 = EB:
+//  * phase 1 (forward stages 0..R1-1, on the row bits): each thread owns one
+//    column, loads its 2^EB words straight from global memory (the 32 lanes
+//    of a warp read 32 consecutive columns: one 128-byte line per
+//    instruction), runs every phase-1 stage in registers and stores the
+//    column back in place.  No shared memory and no barrier;
+//  * one cluster barrier (release / acquire) makes the limb's phase-1 words
+//    visible to the CTAs of the limb;
+//  * phase 2 (stages R1..n-1, on the column bits): CTA r owns the
+//    contiguous rows [r*M, (r+1)*M); its first register pass reads them from
+//    L2 (loads that bypass L1: this SM may hold stale lines of them), the
+//    other passes exchange through the work buffer, and the last one leaves
+//    the canonical words in the work buffer for the coalesced warp-chunk
+//    store (slab_out).
+// The inverse runs the same steps backwards (Gentleman-Sande, the N^{-1}
+// and Montgomery->normal factors folded into the last stage).
+//
+// Why: on B200 a distributed-shared-memory scatter moves 11-15 bytes per SM
+// cycle against ~80 for local shared memory, and ~88% of every limb crossed
+// it; the phase-1 words written back in place stay in the 126 MB L2 (the
+// limbs in flight hold ~22 MB) and are overwritten by the phase-2 output
+// before they are evicted, so HBM traffic stays one read and one write.
+#pragma once
+#include <type_traits>
+
+#include "fused_kernel.cuh"
+
+namespace nttb {
+
+// Extra register bits of the first phase-2 pass: the lowest positions from
+// bit 5 up outside its butterfly range, so that its lanes are bits 0..4.
+template <int MB, int PLO, int KB, int XB>
+constexpr uint32_t split_first_extras() {
+    uint32_t m = 0;
+    for (int p = 5, c = 0; p < MB && c < XB; ++p)
+        if (!(p >= PLO && p < PLO + KB)) {
+            m |= 1u << p;
+            ++c;
+        }
+    return m;
+}
+
+// Geometry of split configuration S(LOGN, CLOG, EB, K2A, K2B) (configs.h).
+template <int LOGN_, int CLOG_, int EB_, int K2A_, int K2B_>
+struct SplitGeo {
+    static constexpr int LOGN = LOGN_, CLOG = CLOG_, EB = EB_, NP = 1;
+    static constexpr int R1 = EB, R2 = LOGN - R1;
+    static constexpr int K2A = K2A_, K2B = K2B_, K2C = R2 - K2A_ - K2B_;
+    static constexpr int C = 1 << CLOG;
+    static constexpr int MB = LOGN - CLOG;
+    static constexpr uint32_t M = 1u << MB;
+    static constexpr int S1 = R2 - CLOG;
+    static constexpr uint32_t W1 = 1u << S1;
+    static constexpr uint32_t H2 = 1u << (R1 - CLOG);
+    static constexpr int TB = MB - EB;
+    static constexpr int THREADS = 1 << TB;
+    static_assert(C > 1 && R1 >= CLOG, "each CTA of the cluster owns at least one row");
+    static_assert(S1 >= 5, "phase-1 lanes take 32 consecutive columns");
+    static_assert(R2 - K2A >= 5, "the first phase-2 pass keeps bits 0..4 for its lanes");
+    static_assert(K2A >= 1 && K2A <= EB && K2B >= 1 && K2B <= EB && K2C >= 0 && K2C <= EB,
+                  "phase-2 passes");
+    static_assert(TB >= 5 && TB <= 10, "32..1024 threads per CTA");
+    static_assert(LOGN < kTwPermMinLogN || R2 >= kTwPermStages,
+                  "the interleaved twiddle stages must all lie in phase 2");
+    // registers: the 2^EB data words plus 16 (measured on B200 for the
+    // cluster kernels: occupancy beats per-thread ILP here)
+    static constexpr int REG_BUDGET = (1 << EB) + 16 > 32 ? (1 << EB) + 16 : 32;
+    static constexpr int MIN_BLOCKS = 65536 / (THREADS * REG_BUDGET) > 0
+                                          ? 65536 / (THREADS * REG_BUDGET) : 1;
+
+    using P1 = PassLayout<MB, MB - EB, EB, EB, 0>;
+    using P2A = PassLayoutX<MB, R2 - K2A, K2A, EB,
+                            split_first_extras<MB, R2 - K2A, K2A, EB - K2A>()>;
+    using P2B = PassLayout<MB, R2 - K2A - K2B, K2B, EB, 0>;
+    using P2C = PassLayout<MB, 0, (K2C > 0 ? K2C : 1), EB, 0>;
+    using PLast = std::conditional_t<(K2C > 0), P2C, P2B>;
+
+    using LT = SplitLayoutTable<LOGN, CLOG, EB, K2A, K2B>;
+    static_assert(LT::lanes_P2A == P2A::kLanes && LT::lanes_P2B == P2B::kLanes,
+                  "layouts_gen.h is stale: rerun gen_layouts.py");
+    using XW = Spread<LT::XW[0], LT::XW[1], LT::XW[2], LT::XW[3]>;
+    static constexpr uint32_t SLAB_WORDS = ((uint32_t)LT::XW[4] + 3u) & ~3u;
+    static constexpr uint32_t SMEM_BYTES = SLAB_WORDS * 4u;
+
+    // exchanges between passes that keep every warp's words stay warp-local
+    static constexpr uint32_t kChunkWarps = ((THREADS / 32u) - 1u) << (MB - (TB - 5));
+    static constexpr bool kABWarp = warp_bits<P2A>() == warp_bits<P2B>();
+    static constexpr bool kBCWarp = warp_bits<P2B>() == warp_bits<P2C>();
+    static constexpr bool kChunkWarp = warp_bits<PLast>() == kChunkWarps;
+};
+
+template <bool WarpLocal>
+__device__ __forceinline__ void split_sync() {
+    if constexpr (WarpLocal) __syncwarp();
+    else __syncthreads();
+}
+
+// The cluster kernels' device context, with global loads that either stream
+// (phase-1 input, read once) or bypass L1 (words other CTAs of the cluster
+// rewrote after this SM may have cached their lines).
+template <int C>
+struct SplitCtx : DevCtx<C, false, 1, false> {
+    bool cg = false;
+    __device__ __forceinline__ uint32_t g_ld(const uint32_t* b, uint32_t c) const {
+        return cg ? __ldcg(b + c) : __ldcs(b + c);
+    }
+    __device__ __forceinline__ void g_ld4(const uint32_t* b, uint32_t c, uint32_t& x, uint32_t& y,
+                                          uint32_t& z, uint32_t& w) const {
+        const uint4* p = reinterpret_cast<const uint4*>(b + c);
+        const uint4 t = cg ? __ldcg(p) : __ldcs(p);
+        x = t.x;
+        y = t.y;
+        z = t.z;
+        w = t.w;
+    }
+};
+
+// The limb's phase-1 words are in place: make them visible to its CTAs.
+__device__ __forceinline__ void split_exchange() {
+    cluster_arrive_release();
+    cluster_wait_acquire();
+}
+
+template <class G, class Arith, class Ctx>
+__device__ __forceinline__ void split_forward_body(Ctx& ctx) {
+    using Mp = Maps<G>;
+    using X = typename G::XW;
+    using P1 = typename G::P1;
+    using P2A = typename G::P2A;
+    using P2B = typename G::P2B;
+    using P2C = typename G::P2C;
+    const uint32_t tid = threadIdx.x;
+    const FwdFinal<Arith> fin{ctx.q, ctx.q2};
+    {
+        uint32_t v[1][P1::E];
+        const uint32_t d = P1::dep(tid);
+        const uint32_t g = Mp::g1(d) + Mp::g1_rank(ctx.rank);
+        load_global<P1, G::W1, G1Map<G>>(ctx, v, g);
+        run_stages<G, P1, Arith, true, false, true>(ctx, v, d);
+        store_global<P1, G::W1, G1Map<G>>(ctx, v, g, Ident{});
+    }
+    split_exchange();
+    ctx.cg = true;
+    {
+        uint32_t v[1][P2A::E];
+        const uint32_t d = P2A::dep(tid);
+        load_global<P2A, (1u << 30), G2Map>(ctx, v, d + ctx.rank * G::M);
+        run_stages<G, P2A, Arith, true, true, false>(ctx, v, d);
+        store_smem<P2A, X, G::SLAB_WORDS>(ctx, v, d);
+    }
+    split_sync<G::kABWarp>();
+    {
+        uint32_t v[1][P2B::E];
+        const uint32_t d = P2B::dep(tid);
+        load_smem<P2B, X, G::SLAB_WORDS>(ctx, v, d);
+        run_stages<G, P2B, Arith, true, true, false>(ctx, v, d);
+        if constexpr (G::K2C == 0)
+            ct_for<P2B::E>([&](auto R) { v[0][decltype(R)::value] = fin(v[0][decltype(R)::value]); });
+        store_smem<P2B, X, G::SLAB_WORDS>(ctx, v, d);
+    }
+    if constexpr (G::K2C > 0) {
+        split_sync<G::kBCWarp>();
+        uint32_t v[1][P2C::E];
+        const uint32_t d = P2C::dep(tid);
+        load_smem<P2C, X, G::SLAB_WORDS>(ctx, v, d);
+        run_stages<G, P2C, Arith, true, true, false>(ctx, v, d);
+        ct_for<P2C::E>([&](auto R) { v[0][decltype(R)::value] = fin(v[0][decltype(R)::value]); });
+        store_smem<P2C, X, G::SLAB_WORDS>(ctx, v, d);
+    }
+    split_sync<G::kChunkWarp>();  // the warp's chunk holds the words it wrote
+    slab_out<G, X>(ctx, tid);
+}
+
+template <class G, class Arith, class Ctx>
+__device__ __forceinline__ void split_inverse_body(Ctx& ctx) {
+    using Mp = Maps<G>;
+    using X = typename G::XW;
+    using P1 = typename G::P1;
+    using P2A = typename G::P2A;
+    using P2B = typename G::P2B;
+    using P2C = typename G::P2C;
+    const uint32_t tid = threadIdx.x;
+    slab_in<G, X>(ctx, tid);
+    split_sync<G::kChunkWarp>();
+    if constexpr (G::K2C > 0) {
+        uint32_t v[1][P2C::E];
+        const uint32_t d = P2C::dep(tid);
+        load_smem<P2C, X, G::SLAB_WORDS>(ctx, v, d);
+        run_stages<G, P2C, Arith, false, true, false>(ctx, v, d);
+        store_smem<P2C, X, G::SLAB_WORDS>(ctx, v, d);
+        split_sync<G::kBCWarp>();
+    }
+    {
+        uint32_t v[1][P2B::E];
+        const uint32_t d = P2B::dep(tid);
+        load_smem<P2B, X, G::SLAB_WORDS>(ctx, v, d);
+        run_stages<G, P2B, Arith, false, true, false>(ctx, v, d);
+        store_smem<P2B, X, G::SLAB_WORDS>(ctx, v, d);
+    }
+    split_sync<G::kABWarp>();
+    {
+        uint32_t v[1][P2A::E];
+        const uint32_t d = P2A::dep(tid);
+        load_smem<P2A, X, G::SLAB_WORDS>(ctx, v, d);
+        run_stages<G, P2A, Arith, false, true, false>(ctx, v, d);
+        store_global<P2A, (1u << 30), G2Map>(ctx, v, d + ctx.rank * G::M, Ident{});
+    }
+    split_exchange();
+    ctx.cg = true;
+    {
+        uint32_t v[1][P1::E];
+        const uint32_t d = P1::dep(tid);
+        const uint32_t g = Mp::g1(d) + Mp::g1_rank(ctx.rank);
+        load_global<P1, G::W1, G1Map<G>>(ctx, v, g);
+        run_stages<G, P1, Arith, false, false, true>(ctx, v, d);
+        store_global<P1, G::W1, G1Map<G>>(ctx, v, g, Ident{});
+    }
+}
+
+// One launch over the limb transforms of a plan: cluster c runs the
+// limb-major jobs [c * jobs_per_cluster, ...) (FusedArgs; one polynomial per
+// job).  Between two jobs of a cluster the next job's cluster barrier orders
+// the previous job's reads of the work buffer before its rewrite.
+template <class G, bool Fwd, class Arith>
+__global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) split_kernel(FusedArgs a) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    const uint32_t rank = cluster_rank();
+    const uint32_t cluster = blockIdx.x / G::C;
+    const uint32_t j0 = cluster * a.jobs_per_cluster;
+    const uint32_t j1 = min(j0 + a.jobs_per_cluster, a.jobs);
+    SplitCtx<G::C> ctx;
+    ctx.smem = smem;
+    ctx.stage = nullptr;
+    ctx.smem_sa = (uint32_t)__cvta_generic_to_shared(smem);
+    ctx.rank = rank;
+    for (uint32_t job = j0; job < j1; ++job) {
+        const uint32_t limb = job / a.polys, poly = job - limb * a.polys;
+        ctx.o[0] = a.data + (size_t)poly * a.poly_stride + ((size_t)limb << G::LOGN);
+        ctx.g[0] = ctx.o[0];
+        ctx.twp = a.tw + ((size_t)limb << G::LOGN);
+        ctx.q = __ldg(a.q + limb);
+        ctx.q2 = 2u * ctx.q;
+        ctx.scale_c = a.scale ? __ldg(a.scale + limb) % ctx.q : kNoScale;
+        ctx.cg = false;
+        if constexpr (Fwd) split_forward_body<G, Arith>(ctx);
+        else split_inverse_body<G, Arith>(ctx);
+    }
+}
+
+}  // namespace nttb

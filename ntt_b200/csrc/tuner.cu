@@ -119,7 +119,7 @@ ntt_status_t ntt_config_get(int index, ntt_kernel_config_t* out) {
     if (!c || !out) return fail(NTT_ERR_INVALID_ARGUMENT, "bad config index %d", index);
     *out = ntt_kernel_config_t{c->logN, 1 << c->clog, c->r1,      c->eb,
                                c->k1a,  c->k2a,       c->threads, c->smem_bytes_direct,
-                               c->np};
+                               c->np,   c->split,     c->split ? c->k2b : 0};
     return NTT_OK;
 }
 

@@ -100,7 +100,14 @@ def test_config_catalogue_covers_every_size():
         assert c.smem_bytes <= 227 * 1024
         assert c.cluster_ctas in (1, 2, 4, 8, 16)
         assert c.polys_per_job in (1, 2)
+        assert c.exchange in (0, 1)
+        if c.exchange:  # split: one phase-1 pass per column, 2 or 3 phase-2 passes
+            assert c.k1a == c.r1 == c.words_log2 and c.polys_per_job == 1
+            k2c = c.logN - c.r1 - c.k2a - c.k2b
+            assert 1 <= c.k2a <= c.words_log2 and 1 <= c.k2b <= c.words_log2
+            assert 0 <= k2c <= c.words_log2
     assert any(c.polys_per_job == 2 for c in cfgs)
+    assert {c.logN for c in cfgs if c.exchange} >= {15, 16, 17}
 
 
 def test_plan_without_device_fails_cleanly():
