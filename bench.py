@@ -454,7 +454,7 @@ def summary(out):
     if "fused_multiply" in out:
         fm = out["fused_multiply"]
         s["multiply_speedup_vs_unfused"] = r(fm["speedup_vs_unfused"])
-        s["multiply_plan_speedup_vs_unfused"] = r(fm["plan_fused"]["speedup_vs_unfused"])
+        s["multiply_batch_tiles_speedup_vs_unfused"] = r(fm["batch_tiles"]["speedup_vs_unfused"])
     if "serve" in out:
         for leg in ("host", "device"):
             L = out["serve"][leg]
@@ -550,13 +550,14 @@ def bench_batched(args, torch, nb, stream):
 def bench_multiply(args, torch, nb, stream):
     """Fused negacyclic multiply: 128 pairs of 2^16 x 24-limb polynomials
     (24 ascending 30-bit primes q == 1 mod 2^17 above 2^29.5), uniform [0, q)
-    coefficients; c = a * b into b's buffer.  Fused: one persistent launch of
-    multiply tiles (NTT(a), NTT(b), pointwise Montgomery product, INTT per
-    limb, a read once, b read and overwritten once).  Unfused: the plain
-    calls forward_many(a), forward_many(b), pointwise_mul, inverse_many(b)
-    (4 launches; a is overwritten by its spectrum, which favours it).  Plan
-    form: multiply_many (3 launches of the plain transform kernels: NTT(b),
-    NTT(a) with the pointwise product folded into its store, INTT(b))."""
+    coefficients; c = a * b into b's buffer.  Fused: ntt_multiply_many, one
+    persistent launch over every (pair, limb) job: NTT(b), NTT(a), the
+    pointwise Montgomery product and INTT per limb, a read once and b read
+    and written once (12 bytes per coefficient).  Unfused: the plain calls
+    forward_many(a), forward_many(b), pointwise_mul, inverse_many(b) (4
+    launches, 36 bytes per coefficient; a is overwritten by its spectrum,
+    which favours it).  Batch tiles: the same products as multiply tiles of
+    the ragged-batch kernel (one launch; the serving path's form)."""
     from ntt_b200 import mixes
     logN, limbs, pairs = 16, 24, 128
     mods = list(mixes.prime_pool(logN, 30, limbs))
@@ -567,25 +568,25 @@ def bench_multiply(args, torch, nb, stream):
     b = torch.stack([mixes.uniform_device(torch, job, g) for _ in range(pairs)])
     sh = stream.cuda_stream
     p = nb.Plan(logN, mods)
-    fused = nb.Batch([(nb.OP_MULTIPLY, logN, mods, b[i], a[i]) for i in range(pairs)])
-    # consistency of the two forms on this workload (parity is the tests' job)
+    tiles = nb.Batch([(nb.OP_MULTIPLY, logN, mods, b[i], a[i]) for i in range(pairs)])
+    # consistency of the forms on this workload (parity is the tests' job)
     b0 = b.clone()
     ta, tb = a.clone(), b.clone()
     with torch.cuda.stream(stream):
-        fused.run(sh)
         p.forward_many(ta, pairs, 0, sh)
         p.forward_many(tb, pairs, 0, sh)
         p.pointwise_mul(tb, ta, tb, pairs, 0, sh)
         p.inverse_many(tb, pairs, 0, sh)
+        tiles.run(sh)
     stream.synchronize()
     if not torch.equal(b, tb):
-        raise RuntimeError("fused and unfused multiply differ")
+        raise RuntimeError("batch-tile and unfused multiply differ")
     pb = b0.clone()
     with torch.cuda.stream(stream):
         p.multiply_many(a, pb, pairs, 0, sh)
     stream.synchronize()
     if not torch.equal(pb, tb):
-        raise RuntimeError("plan-level and unfused multiply differ")
+        raise RuntimeError("fused and unfused multiply differ")
     del b0
 
     def unfused():
@@ -595,10 +596,10 @@ def bench_multiply(args, torch, nb, stream):
         p.inverse_many(tb, pairs, 0, sh)
 
     w = 3
-    fused_ms = device_time(torch, stream, lambda: fused.run(sh), args.multiply_steps, w)
+    fused_ms = device_time(torch, stream, lambda: p.multiply_many(a, pb, pairs, 0, sh),
+                           args.multiply_steps, w)
     unfused_ms = device_time(torch, stream, unfused, args.multiply_steps, w)
-    plan_ms = device_time(torch, stream, lambda: p.multiply_many(a, pb, pairs, 0, sh),
-                          args.multiply_steps, w)
+    tiles_ms = device_time(torch, stream, lambda: tiles.run(sh), args.multiply_steps, w)
     products = pairs * limbs
     words = pairs * limbs << logN
     res = {
@@ -607,19 +608,18 @@ def bench_multiply(args, torch, nb, stream):
         "value": products / (fused_ms / 1000.0), "unit": "limb-products/s",
         "limb_ntt_per_s": 3 * products / (fused_ms / 1000.0),
         "ms_per_step": fused_ms, "launches_per_step": 1,
+        "form": "ntt_multiply_many: one persistent launch (NTT(b), NTT(a), product, INTT per limb)",
         "algorithmic_bytes": 12 * words,
         "achieved_gbs": 12 * words / (fused_ms / 1000.0) / 1e9,
         "unfused": {"value": products / (unfused_ms / 1000.0), "ms_per_step": unfused_ms,
                     "launches_per_step": 4, "algorithmic_bytes": 36 * words},
         "speedup_vs_unfused": unfused_ms / fused_ms,
-        "plan_fused": {"value": products / (plan_ms / 1000.0), "ms_per_step": plan_ms,
-                       "launches_per_step": 3, "algorithmic_bytes": 24 * words,
-                       "speedup_vs_unfused": unfused_ms / plan_ms},
-        "kernel": {"cluster_ctas": fused.info.cluster_ctas, "clusters": fused.info.clusters,
-                   "smem_bytes": fused.info.smem_bytes},
+        "batch_tiles": {"value": products / (tiles_ms / 1000.0), "ms_per_step": tiles_ms,
+                        "launches_per_step": 1, "speedup_vs_unfused": unfused_ms / tiles_ms,
+                        "cluster_ctas": tiles.info.cluster_ctas, "clusters": tiles.info.clusters},
         "steps": args.multiply_steps, "warmup": w,
     }
-    fused.close()
+    tiles.close()
     p.close()
     return res
 

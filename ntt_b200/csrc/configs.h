@@ -61,6 +61,10 @@ struct FusedConfig {
     const void* kern_mul[2];
     int split;  // 1: split configuration (exchange through L2), 0: cluster scatter
     int k2b;    // split: stages of the second phase-2 pass
+    // split: the one-launch negacyclic product (split_mul_kernel) [lazy2]
+    // and its dynamic shared memory (work buffer + the spectrum of b)
+    const void* kern_smul[2];
+    uint32_t smem_smul;
     bool has_mul() const { return kern_mul[0] != nullptr; }
     const void* kernel(bool staged, bool fwd, bool lazy2) const {
         return kern[staged ? 1 : 0][fwd ? 1 : 0][lazy2 ? 1 : 0];

@@ -1,7 +1,7 @@
 // FusedConfig table entry of split configuration S(N, CL, EB, K2A, K2B)
-// (configs.h, split_kernel.cuh): the kernel loops over its cluster's jobs, so
-// the direct and the staged schedule run the same kernel; the forward with
-// the product epilogue is left to a cluster configuration (kern_mul null).
+// (configs.h, split_kernel.cuh): one job per cluster, so both schedules run
+// the same direct launch; the forward with the product epilogue is left to a
+// cluster configuration (kern_mul null); kern_smul is the one-launch product.
 #pragma once
 #include "../configs.h"
 #include "../split_kernel.cuh"
@@ -15,4 +15,7 @@
        {NTTB_SK(N, CL, EB, KA, KB, true, Lazy4), NTTB_SK(N, CL, EB, KA, KB, true, Lazy2)}},      \
       {{NTTB_SK(N, CL, EB, KA, KB, false, Lazy4), NTTB_SK(N, CL, EB, KA, KB, false, Lazy2)},     \
        {NTTB_SK(N, CL, EB, KA, KB, true, Lazy4), NTTB_SK(N, CL, EB, KA, KB, true, Lazy2)}}},     \
-     {nullptr, nullptr}, 1, KB},
+     {nullptr, nullptr}, 1, KB,                                                                  \
+     {(const void*)&split_mul_kernel<NTTB_SG(N, CL, EB, KA, KB), Lazy4>,                         \
+      (const void*)&split_mul_kernel<NTTB_SG(N, CL, EB, KA, KB), Lazy2>},                        \
+     SplitMulGeo<NTTB_SG(N, CL, EB, KA, KB)>::SMEM_BYTES},

@@ -272,7 +272,9 @@ def split_layout(cfg):
     cands += [(a1, c1, a2, c2) for a1 in range(MB) for c1 in cs
               for a2 in range(a1 + 1, MB) for c2 in cs]
     for lay in cands:
-        if phys(top, *lay) + 1 > (top + 1) * 9 // 8:
+        # up to 1/4 of pads: 5 CTAs of 256 threads still fit an SM's shared
+        # memory (the split kernels hold one buffer per CTA)
+        if phys(top, *lay) + 1 > (top + 1) * 5 // 4:
             continue
         worst, cost = 1, 0
         for name, pos, run, both in ps:  # the first pass only stores

@@ -213,7 +213,7 @@ struct SplitLayoutTable;
 
 template <>
 struct SplitLayoutTable<16, 3, 5, 4, 4> {
-    static constexpr int XW[5] = {5, 2, 13, 0, 8702};
+    static constexpr int XW[5] = {5, 4, 8, 8, 9460};
     static constexpr uint32_t lanes_P2A = 0x1fu;
     static constexpr uint32_t lanes_P2B = 0x386u;
     static constexpr uint32_t lanes_P2C = 0x3e0u;
@@ -221,7 +221,7 @@ struct SplitLayoutTable<16, 3, 5, 4, 4> {
 
 template <>
 struct SplitLayoutTable<16, 3, 4, 4, 4> {
-    static constexpr int XW[5] = {5, 2, 13, 0, 8702};
+    static constexpr int XW[5] = {5, 4, 8, 16, 9708};
     static constexpr uint32_t lanes_P2A = 0x1fu;
     static constexpr uint32_t lanes_P2B = 0x10fu;
     static constexpr uint32_t lanes_P2C = 0x1f0u;
@@ -229,7 +229,7 @@ struct SplitLayoutTable<16, 3, 4, 4, 4> {
 
 template <>
 struct SplitLayoutTable<17, 4, 5, 4, 4> {
-    static constexpr int XW[5] = {5, 2, 13, 0, 8702};
+    static constexpr int XW[5] = {5, 4, 8, 16, 9708};
     static constexpr uint32_t lanes_P2A = 0x1fu;
     static constexpr uint32_t lanes_P2B = 0x30eu;
     static constexpr uint32_t lanes_P2C = 0x3e0u;
@@ -244,7 +244,7 @@ struct SplitLayoutTable<15, 2, 5, 5, 5> {
 
 template <>
 struct SplitLayoutTable<15, 2, 4, 4, 4> {
-    static constexpr int XW[5] = {5, 2, 13, 0, 8702};
+    static constexpr int XW[5] = {5, 4, 8, 8, 9460};
     static constexpr uint32_t lanes_P2A = 0x1fu;
     static constexpr uint32_t lanes_P2B = 0x187u;
     static constexpr uint32_t lanes_P2C = 0x1f0u;
