@@ -721,3 +721,69 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# ---------------------------------------------------------------------------
+# 64-bit words (include/ntt_b200_u64.h)
+# ---------------------------------------------------------------------------
+
+
+class ModulusConfig64(ctypes.Structure):
+    _fields_ = [("qi", ctypes.c_uint64), ("primitive_root", ctypes.c_uint64)]
+
+    def __iter__(self):
+        return iter((self.qi, self.primitive_root))
+
+
+_sig("ntt64_find_moduli", _st, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+     ctypes.POINTER(ModulusConfig64))
+_sig("ntt64_plan_create", _st, ctypes.c_int, ctypes.POINTER(ModulusConfig64), ctypes.c_int,
+     ctypes.POINTER(_vp))
+_sig("ntt64_plan_destroy", _st, _vp)
+_sig("ntt64_forward_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
+_sig("ntt64_inverse_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
+
+
+def find_moduli64(logN: int, count: int, lower_bound: int) -> List[ModulusConfig64]:
+    """First `count` primes >= lower_bound with q == 1 (mod 2N), q < 2^62,
+    ascending, each with its smallest quadratic non-residue as root."""
+    arr = (ModulusConfig64 * max(1, count))()
+    _check(_lib.ntt64_find_moduli(logN, count, lower_bound, arr), "ntt64_find_moduli")
+    return list(arr)[:count]
+
+
+class Plan64:
+    """64-bit word plan: limbs * 2^logN uint64 words per polynomial (torch
+    int64 / uint64 CUDA tensors), the 32-bit plans' domain contract with
+    R = 2^64."""
+
+    def __init__(self, logN: int, moduli: Sequence):
+        m = (ModulusConfig64 * len(moduli))(*[ModulusConfig64(int(q), int(g)) for q, g in moduli])
+        h = _vp()
+        _check(_lib.ntt64_plan_create(logN, m, len(moduli), ctypes.byref(h)), "ntt64_plan_create")
+        self._h, self.logN, self.limbs = h, logN, len(moduli)
+
+    def forward_many(self, a, polys: int = 1, poly_stride: int = 0, stream=None):
+        _check(_lib.ntt64_forward_many(self._h, _ptr(a), polys, poly_stride, _stream(stream)),
+               "ntt64_forward_many")
+
+    def inverse_many(self, a, polys: int = 1, poly_stride: int = 0, stream=None):
+        _check(_lib.ntt64_inverse_many(self._h, _ptr(a), polys, poly_stride, _stream(stream)),
+               "ntt64_inverse_many")
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.ntt64_plan_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,346 @@
+// 64-bit word variant of the RNS negacyclic NTT / INTT (include/ntt_b200_u64.h).
+//
+// Same algorithm and table conventions as the 32-bit path (reference:
+// cpu_ntt_butterfly / cpu_intt_butterfly and the two-phase kernels of
+// src/v04_montgomery.cu:196-580, 742-784) with 64-bit words: Shoup products
+// w*a - umulhi(w', a)*q (w' = floor(w * 2^64 / q)) and Harvey's lazy ranges,
+// so q < 2^62.  The Montgomery factor R = 2^64 and N^{-1} ride on the
+// stage-0 twiddle pair (table entries 0 and 1), as in the 32-bit tables.
+//
+// Kernel: one stage-range kernel.  A CTA loads G sub-transforms of 2^k
+// words of a limb into shared memory (G adjacent columns of the 2^k x
+// 2^(n-k) limb matrix for the column stages, or G adjacent rows for the row
+// stages; both loads coalesced), runs the launch's radix-2 stages there, and
+// writes the words back in place.  logN <= 12: one launch with all stages on
+// whole limbs; larger: the column stages, then the row stages.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <vector>
+
+#include "../../include/ntt_b200_u64.h"
+#include "runtime.h"
+
+using namespace nttb;
+
+namespace {
+
+typedef unsigned __int128 u128;
+
+struct TwPair64 {
+    unsigned long long w, wp;
+};
+
+// ---- host arithmetic -------------------------------------------------------
+uint64_t mulmod64(uint64_t a, uint64_t b, uint64_t q) { return (uint64_t)((u128)a * b % q); }
+uint64_t powmod64(uint64_t a, uint64_t e, uint64_t q) {
+    uint64_t r = 1 % q;
+    a %= q;
+    for (; e; e >>= 1, a = mulmod64(a, a, q))
+        if (e & 1) r = mulmod64(r, a, q);
+    return r;
+}
+// Deterministic Miller-Rabin for n < 2^64 (the first 12 primes as bases).
+bool is_prime64(uint64_t n) {
+    if (n < 2) return false;
+    static const uint64_t bases[] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+    for (uint64_t p : bases)
+        if (n % p == 0) return n == p;
+    uint64_t d = n - 1;
+    int s = 0;
+    while ((d & 1) == 0) {
+        d >>= 1;
+        ++s;
+    }
+    for (uint64_t a : bases) {
+        uint64_t x = powmod64(a, d, n);
+        if (x == 1 || x == n - 1) continue;
+        bool comp = true;
+        for (int r = 1; r < s && comp; ++r) {
+            x = mulmod64(x, x, n);
+            if (x == n - 1) comp = false;
+        }
+        if (comp) return false;
+    }
+    return true;
+}
+uint32_t bitrev(uint32_t x, int bits) {
+    uint32_t r = 0;
+    for (int i = 0; i < bits; ++i) r |= ((x >> i) & 1u) << (bits - 1 - i);
+    return r;
+}
+TwPair64 pair_of(uint64_t w, uint64_t q) { return TwPair64{w, (uint64_t)(((u128)w << 64) / q)}; }
+
+// ---- device arithmetic (lazy ranges as Lazy4 in arith.cuh) ------------------
+__device__ __forceinline__ uint64_t csub64(uint64_t x, uint64_t m) {
+    const uint64_t y = x - m;
+    return y < x ? y : x;  // x >= m: x - m; else the subtraction wrapped
+}
+__device__ __forceinline__ uint64_t shoup64(uint64_t a, TwPair64 w, uint64_t q) {
+    return a * w.w - __umul64hi(a, w.wp) * q;  // in [0, 2q)
+}
+
+struct U64Args {
+    unsigned long long* data;
+    const TwPair64* tw;  // [limbs][N]
+    const unsigned long long* q;
+    unsigned long long stride;  // words between polynomials
+    uint32_t limbs, groups;     // sub-transform groups per limb
+    int n, k, s0, s1;           // logN, log2 local size, global stages [s0, s1)
+    int col;                    // 1: column stages (stride 2^(n-k)), 0: rows
+    int G;                      // sub-transforms per CTA
+};
+
+// Global word offset (within the limb) of local word u of sub-transform c.
+__device__ __forceinline__ uint32_t u64_off(const U64Args& a, uint32_t c, uint32_t u) {
+    return a.col ? c + (u << (a.n - a.k)) : (c << a.k) + u;
+}
+
+template <bool Fwd>
+__global__ void __launch_bounds__(256) u64_stage_kernel(U64Args a) {
+    extern __shared__ unsigned long long s[];
+    const uint32_t group = blockIdx.x % a.groups;
+    const uint32_t lp = blockIdx.x / a.groups;  // limb-major: limb * polys + poly
+    const uint32_t polys = gridDim.x / (a.groups * a.limbs);
+    const uint32_t limb = lp / polys, poly = lp - limb * polys;
+    unsigned long long* x = a.data + poly * a.stride + ((size_t)limb << a.n);
+    const TwPair64* tw = a.tw + ((size_t)limb << a.n);
+    const uint64_t q = a.q[limb], q2 = 2 * q;
+    const uint32_t K = 1u << a.k, G = (uint32_t)a.G, total = G * K;
+    const uint32_t c0 = group * G;
+    // load: consecutive indices are consecutive words in global memory
+    for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
+        uint32_t g, u, si;
+        if (a.col) { u = i / G; g = i - u * G; si = i; }
+        else { g = i >> a.k; u = i & (K - 1); si = i; }
+        s[si] = x[u64_off(a, c0 + g, u)];
+    }
+    __syncthreads();
+    const uint32_t half = total >> 1;
+    for (int st = 0; st < a.s1 - a.s0; ++st) {
+        const int sg = Fwd ? a.s0 + st : a.s1 - 1 - st;  // global stage
+        const int b = a.col ? a.k - 1 - sg : a.n - 1 - sg;  // local bit
+        for (uint32_t bf = threadIdx.x; bf < half; bf += blockDim.x) {
+            const uint32_t g = bf >> (a.k - 1), p = bf & ((K >> 1) - 1);
+            const uint32_t u = ((p >> b) << (b + 1)) | (p & ((1u << b) - 1));
+            const uint32_t v = u + (1u << b);
+            const uint32_t su = a.col ? u * G + g : (g << a.k) + u;
+            const uint32_t sv = a.col ? v * G + g : (g << a.k) + v;
+            uint64_t X = s[su], Y = s[sv];
+            const uint32_t gi = u64_off(a, c0 + g, u);
+            if (sg == 0) {
+                const TwPair64 f = tw[0], fw = tw[1];
+                if (Fwd) {
+                    const uint64_t A = shoup64(X, f, q), T = shoup64(Y, fw, q);
+                    X = A + T;
+                    Y = A - T + q2;
+                } else {
+                    const uint64_t S = X + Y, D = X - Y + q2;
+                    X = csub64(shoup64(S, f, q), q);
+                    Y = csub64(shoup64(D, fw, q), q);
+                }
+            } else {
+                const TwPair64 w = tw[(1u << sg) + (gi >> (a.n - sg))];
+                if (Fwd) {
+                    const uint64_t A = csub64(X, q2), T = shoup64(Y, w, q);
+                    X = A + T;
+                    Y = A - T + q2;
+                } else {
+                    const uint64_t S = X + Y, D = X - Y + q2;
+                    X = csub64(S, q2);
+                    Y = shoup64(D, w, q);
+                }
+            }
+            s[su] = X;
+            s[sv] = Y;
+        }
+        __syncthreads();
+    }
+    const bool canon = Fwd && a.s1 == a.n;  // the forward's last stage: canonical words
+    for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
+        uint32_t g, u;
+        if (a.col) { u = i / G; g = i - u * G; }
+        else { g = i >> a.k; u = i & (K - 1); }
+        uint64_t v = s[i];
+        if (canon) v = csub64(csub64(v, q2), q);
+        x[u64_off(a, c0 + g, u)] = v;
+    }
+}
+
+}  // namespace
+
+struct ntt64_plan {
+    int logN = 0, limbs = 0, device = 0;
+    TwPair64* fwd = nullptr;  // [limbs][N] device, then inv, then q
+    TwPair64* inv = nullptr;
+    unsigned long long* q = nullptr;
+    void* block = nullptr;
+};
+
+namespace {
+
+ntt_status_t validate64(int logN, ModulusConfig64 m, uint64_t* psi) {
+    const uint64_t N = uint64_t{1} << logN, q = m.qi;
+    if (q < 3 || (q - 1) % (2 * N) != 0)
+        return fail(NTT_ERR_MODULUS, "q must satisfy q == 1 mod 2N (q=%llu, logN=%d)",
+                    (unsigned long long)q, logN);
+    if (q >> 62) return fail(NTT_ERR_MODULUS_RANGE, "modulus %llu must be below 2^62", (unsigned long long)q);
+    if (!is_prime64(q)) return fail(NTT_ERR_MODULUS_RANGE, "modulus %llu is not prime", (unsigned long long)q);
+    const uint64_t p = powmod64(m.primitive_root, (q - 1) / (2 * N), q);
+    if (powmod64(p, N, q) != q - 1)
+        return fail(NTT_ERR_ROOT, "root %llu does not give a primitive 2N-th root mod %llu",
+                    (unsigned long long)m.primitive_root, (unsigned long long)q);
+    *psi = p;
+    return NTT_OK;
+}
+
+// Forward and inverse tables of one limb: tw[i] = psi^bitrev(i) with Shoup
+// companions; entries 0 and 1 carry R (forward stage 0) and N^{-1} R^{-1}
+// (inverse last stage), R = 2^64 mod q.
+void limb_tables(int logN, uint64_t q, uint64_t psi, TwPair64* f, TwPair64* iv) {
+    const uint32_t N = 1u << logN;
+    const uint64_t psi_inv = powmod64(psi, q - 2, q);
+    std::vector<uint64_t> pw(N), pwi(N);
+    pw[0] = pwi[0] = 1;
+    for (uint32_t k = 1; k < N; ++k) {
+        pw[k] = mulmod64(pw[k - 1], psi, q);
+        pwi[k] = mulmod64(pwi[k - 1], psi_inv, q);
+    }
+    for (uint32_t i = 0; i < N; ++i) {
+        f[i] = pair_of(pw[bitrev(i, logN)], q);
+        iv[i] = pair_of(pwi[bitrev(i, logN)], q);
+    }
+    const uint64_t R = (uint64_t)(((u128)1 << 64) % q);
+    const uint64_t c = mulmod64(powmod64(N % q, q - 2, q), powmod64(R, q - 2, q), q);
+    f[0] = pair_of(R, q);
+    if (N > 1) f[1] = pair_of(mulmod64(pw[bitrev(1, logN)], R, q), q);
+    iv[0] = pair_of(c, q);
+    if (N > 1) iv[1] = pair_of(mulmod64(pwi[bitrev(1, logN)], c, q), q);
+}
+
+ntt_status_t run64(const ntt64_plan* p, uint64_t* a, size_t polys, size_t stride, bool fwd,
+                   cudaStream_t s) {
+    if (!p || !a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (polys == 0) return NTT_OK;
+    const int n = p->logN;
+    if (stride == 0) stride = (size_t)p->limbs << n;
+    if (polys > 1 && stride < ((size_t)p->limbs << n))
+        return fail(NTT_ERR_INVALID_ARGUMENT, "poly_stride smaller than limbs * N");
+    if (((uintptr_t)a & 15u) || (polys > 1 && (stride & 1u)))
+        return fail(NTT_ERR_MISALIGNED, "data must be 16-byte aligned (stride even)");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaGetDevice");
+    if (dev != p->device)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "plan was created on device %d, current is %d",
+                    p->device, dev);
+    U64Args base{(unsigned long long*)a, fwd ? p->fwd : p->inv, p->q,
+                 (unsigned long long)stride, (uint32_t)p->limbs, 1, n, n, 0, n, 0, 1};
+    std::vector<U64Args> launches;
+    if (n <= 12) {
+        launches.push_back(base);
+    } else {
+        const int k1 = n / 2, k2 = n - k1;
+        U64Args c = base, r = base;
+        c.col = 1;
+        c.k = k1;
+        c.s0 = 0;
+        c.s1 = k1;
+        c.G = std::min(1 << (n - k1), 4096 >> k1);
+        c.groups = (1u << (n - k1)) / c.G;
+        r.col = 0;
+        r.k = k2;
+        r.s0 = k1;
+        r.s1 = n;
+        r.G = 4096 >> k2;
+        r.groups = (1u << k1) / r.G;
+        if (fwd) launches = {c, r};
+        else launches = {r, c};
+    }
+    for (const U64Args& L : launches) {
+        const size_t blocks = (size_t)L.groups * p->limbs * polys;
+        if (blocks > (size_t)INT_MAX) return fail(NTT_ERR_INVALID_ARGUMENT, "too many limbs");
+        const size_t smem = ((size_t)L.G << L.k) * 8;
+        if (fwd) u64_stage_kernel<true><<<(unsigned)blocks, 256, smem, s>>>(L);
+        else u64_stage_kernel<false><<<(unsigned)blocks, 256, smem, s>>>(L);
+        if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return cuda_fail(e, "64-bit NTT launch");
+    }
+    return NTT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ntt_status_t ntt64_find_moduli(int logN, int count, uint64_t lower_bound, ModulusConfig64* out) {
+    if (logN < NTT64_MIN_LOGN || logN > NTT64_MAX_LOGN)
+        return fail(NTT_ERR_UNSUPPORTED, "logN %d outside [%d, %d]", logN, NTT64_MIN_LOGN, NTT64_MAX_LOGN);
+    if (count < 0 || (count > 0 && !out)) return fail(NTT_ERR_INVALID_ARGUMENT, "bad output array");
+    const uint64_t step = uint64_t{2} << logN;
+    uint64_t q = lower_bound <= 1 ? 1 : ((lower_bound - 2) / step + 1) * step + 1;
+    for (int found = 0; found < count; q += step) {
+        if (q >> 62) return fail(NTT_ERR_MODULUS_RANGE, "no more primes below 2^62");
+        if (!is_prime64(q)) continue;
+        uint64_t g = 2;
+        while (powmod64(g, (q - 1) / 2, q) != q - 1) ++g;
+        out[found++] = ModulusConfig64{q, g};
+    }
+    return NTT_OK;
+}
+
+ntt_status_t ntt64_plan_create(int logN, const ModulusConfig64* moduli, int limbs,
+                               ntt64_plan_t** out) {
+    if (!out) return fail(NTT_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (logN < NTT64_MIN_LOGN || logN > NTT64_MAX_LOGN)
+        return fail(NTT_ERR_UNSUPPORTED, "logN %d outside [%d, %d]", logN, NTT64_MIN_LOGN, NTT64_MAX_LOGN);
+    if (limbs < 1 || !moduli) return fail(NTT_ERR_INVALID_ARGUMENT, "need at least one modulus");
+    const size_t N = size_t{1} << logN;
+    std::vector<TwPair64> f(N * limbs), iv(N * limbs);
+    std::vector<unsigned long long> q(limbs);
+    for (int l = 0; l < limbs; ++l) {
+        uint64_t psi = 0;
+        if (ntt_status_t st = validate64(logN, moduli[l], &psi)) return st;
+        limb_tables(logN, moduli[l].qi, psi, f.data() + l * N, iv.data() + l * N);
+        q[l] = moduli[l].qi;
+    }
+    auto* p = new ntt64_plan;
+    p->logN = logN;
+    p->limbs = limbs;
+    cudaGetDevice(&p->device);
+    const size_t tb = N * limbs * sizeof(TwPair64);
+    cudaError_t e = cudaMalloc(&p->block, 2 * tb + limbs * 8);
+    if (e == cudaSuccess) {
+        p->fwd = (TwPair64*)p->block;
+        p->inv = (TwPair64*)((char*)p->block + tb);
+        p->q = (unsigned long long*)((char*)p->block + 2 * tb);
+        e = cudaMemcpy(p->fwd, f.data(), tb, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(p->inv, iv.data(), tb, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(p->q, q.data(), limbs * 8, cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) {
+        if (p->block) cudaFree(p->block);
+        delete p;
+        return cuda_fail(e, "64-bit plan tables");
+    }
+    *out = p;
+    return NTT_OK;
+}
+
+ntt_status_t ntt64_plan_destroy(ntt64_plan_t* p) {
+    if (!p) return NTT_OK;
+    if (p->block) cudaFree(p->block);
+    delete p;
+    return NTT_OK;
+}
+
+ntt_status_t ntt64_forward_many(const ntt64_plan_t* p, uint64_t* a, size_t polys, size_t stride,
+                                ntt_stream_t s) {
+    return run64(p, a, polys, stride, true, (cudaStream_t)s);
+}
+
+ntt_status_t ntt64_inverse_many(const ntt64_plan_t* p, uint64_t* a, size_t polys, size_t stride,
+                                ntt_stream_t s) {
+    return run64(p, a, polys, stride, false, (cudaStream_t)s);
+}
+
+}  // extern "C"

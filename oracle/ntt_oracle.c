@@ -324,3 +324,82 @@ int oracle_transform_limbs(uint32_t* a, int logN, int limbs, const uint32_t* q,
     for (int t = 1; t < threads; ++t) pthread_join(tid[t], NULL);
     return ORACLE_OK;
 }
+
+/* ---- 64-bit words (the 64-bit variant, include/ntt_b200_u64.h) -------------
+ * The same textbook CT NTT / GS INTT as oracle_ntt / oracle_intt (v04:742-784)
+ * with 64-bit words and 128-bit products, and the same O(N^2) definition.
+ * The reference has no 64-bit CPU path in its checkout; these restate the
+ * 32-bit algorithm for q < 2^62 and are pinned by the direct evaluation. */
+typedef unsigned __int128 oracle_u128;
+
+uint64_t oracle_mul_mod64(uint64_t a, uint64_t b, uint64_t q) {
+    return (uint64_t)((oracle_u128)a * b % q);
+}
+
+uint64_t oracle_pow_mod64(uint64_t base, uint64_t exp, uint64_t q) {
+    uint64_t r = 1 % q;
+    base %= q;
+    while (exp) {
+        if (exp & 1) r = oracle_mul_mod64(r, base, q);
+        base = oracle_mul_mod64(base, base, q);
+        exp >>= 1;
+    }
+    return r;
+}
+
+/* psi = g^((q-1)/2N) and the bit-reversed tables of psi and psi^{-1}. */
+void oracle_tables64(int logN, uint64_t q, uint64_t g, uint64_t* psi_tab, uint64_t* inv_tab,
+                     uint64_t* degree_inv) {
+    size_t N = (size_t)1 << logN;
+    uint64_t psi = oracle_pow_mod64(g, (q - 1) / (2 * N), q);
+    uint64_t psi_inv = oracle_pow_mod64(psi, q - 2, q);
+    for (size_t i = 0; i < N; ++i) {
+        uint32_t e = oracle_bit_reverse((uint32_t)i, logN);
+        psi_tab[i] = oracle_pow_mod64(psi, e, q);
+        inv_tab[i] = oracle_pow_mod64(psi_inv, e, q);
+    }
+    *degree_inv = oracle_pow_mod64(N % q, q - 2, q);
+}
+
+void oracle_ntt64(uint64_t* a, int logN, uint64_t q, const uint64_t* psi) {
+    size_t N = (size_t)1 << logN, t = N >> 1;
+    for (size_t m = 1; m < N; m *= 2) {
+        for (size_t j = 0; j < m; ++j)
+            for (size_t k = j * 2 * t; k < j * 2 * t + t; ++k) {
+                uint64_t u = a[k], v = oracle_mul_mod64(a[k + t], psi[m + j], q);
+                a[k] = u + v >= q ? u + v - q : u + v;
+                a[k + t] = u >= v ? u - v : u + q - v;
+            }
+        t >>= 1;
+    }
+}
+
+void oracle_intt64(uint64_t* a, int logN, uint64_t q, const uint64_t* inv_psi,
+                   uint64_t degree_inv) {
+    size_t N = (size_t)1 << logN, t = 1;
+    for (size_t m = N >> 1; m >= 1; m >>= 1) {
+        for (size_t j = 0; j < m; ++j)
+            for (size_t k = j * 2 * t; k < j * 2 * t + t; ++k) {
+                uint64_t u = a[k], v = a[k + t];
+                a[k] = u + v >= q ? u + v - q : u + v;
+                a[k + t] = oracle_mul_mod64(u >= v ? u - v : u + q - v, inv_psi[m + j], q);
+            }
+        t <<= 1;
+        if (m == 1) break;
+    }
+    for (size_t i = 0; i < N; ++i) a[i] = oracle_mul_mod64(a[i], degree_inv, q);
+}
+
+/* out[j] = sum_i a[i] psi^((2 bitrev(j) + 1) i) mod q. */
+void oracle_ntt_direct64(const uint64_t* a, uint64_t* out, int logN, uint64_t q, uint64_t psi) {
+    size_t N = (size_t)1 << logN;
+    for (size_t j = 0; j < N; ++j) {
+        uint64_t step = oracle_pow_mod64(psi, 2ull * oracle_bit_reverse((uint32_t)j, logN) + 1, q);
+        uint64_t w = 1, acc = 0;
+        for (size_t i = 0; i < N; ++i) {
+            acc = (acc + oracle_mul_mod64(a[i], w, q)) % q;
+            w = oracle_mul_mod64(w, step, q);
+        }
+        out[j] = acc;
+    }
+}

@@ -316,3 +316,118 @@ REFERENCE_DEFAULT_MODULI = [
     (957349889, 6), (1073872897, 7), (1209139201, 31), (994705409, 3),
     (998244353, 3), (1073479681, 11), (1158676481, 3), (1016463361, 38),
 ]
+
+
+# ---- 64-bit words (oracle for the 64-bit variant) ----------------------------
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+
+def _p64(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u64p)
+
+
+def _lib64():
+    L = lib()
+    if not getattr(L, "_sig64", False):
+        L.oracle_mul_mod64.restype = ctypes.c_uint64
+        L.oracle_mul_mod64.argtypes = [ctypes.c_uint64] * 3
+        L.oracle_pow_mod64.restype = ctypes.c_uint64
+        L.oracle_pow_mod64.argtypes = [ctypes.c_uint64] * 3
+        L.oracle_tables64.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, _u64p, _u64p,
+                                      _u64p]
+        L.oracle_ntt64.argtypes = [_u64p, ctypes.c_int, ctypes.c_uint64, _u64p]
+        L.oracle_intt64.argtypes = [_u64p, ctypes.c_int, ctypes.c_uint64, _u64p, ctypes.c_uint64]
+        L.oracle_ntt_direct64.argtypes = [_u64p, _u64p, ctypes.c_int, ctypes.c_uint64,
+                                          ctypes.c_uint64]
+        L._sig64 = True
+    return L
+
+
+class LimbTables64:
+    """Per-limb 64-bit tables and the CPU transforms of the 64-bit variant:
+    forward_mont (CPU NTT, then x * 2^64 mod q) and its inverse."""
+
+    def __init__(self, logN: int, moduli: Sequence):
+        L = _lib64()
+        self.logN, self.moduli = logN, [(int(q), int(g)) for q, g in moduli]
+        N = 1 << logN
+        self.q = np.array([q for q, _ in self.moduli], dtype=np.uint64)
+        self.psi_tab = np.zeros((len(moduli), N), dtype=np.uint64)
+        self.inv_tab = np.zeros((len(moduli), N), dtype=np.uint64)
+        self.degree_inv = []
+        for i, (q, g) in enumerate(self.moduli):
+            di = ctypes.c_uint64()
+            L.oracle_tables64(logN, q, g, _p64(self.psi_tab[i]), _p64(self.inv_tab[i]),
+                              ctypes.byref(di))
+            self.degree_inv.append(di.value)
+        self.psi = [pow(g, (q - 1) // (2 * N), q) for q, g in self.moduli]
+
+    def forward(self, a: np.ndarray) -> np.ndarray:
+        out = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        for i, (q, _) in enumerate(self.moduli):
+            _lib64().oracle_ntt64(_p64(out[i]), self.logN, q, _p64(self.psi_tab[i]))
+        return out
+
+    def inverse(self, a: np.ndarray) -> np.ndarray:
+        out = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        for i, (q, _) in enumerate(self.moduli):
+            _lib64().oracle_intt64(_p64(out[i]), self.logN, q, _p64(self.inv_tab[i]),
+                                   self.degree_inv[i])
+        return out
+
+    def direct(self, a: np.ndarray) -> np.ndarray:
+        out = np.zeros_like(a, dtype=np.uint64)
+        for i, (q, _) in enumerate(self.moduli):
+            row = np.ascontiguousarray(a[i], dtype=np.uint64)
+            _lib64().oracle_ntt_direct64(_p64(row), _p64(out[i]), self.logN, q, self.psi[i])
+        return out
+
+    def forward_mont(self, a: np.ndarray) -> np.ndarray:
+        f = self.forward(a)
+        return np.stack([np.array([(int(v) << 64) % q for v in f[i]], dtype=np.uint64)
+                         for i, (q, _) in enumerate(self.moduli)])
+
+    def to_mont(self, a: np.ndarray) -> np.ndarray:
+        return np.stack([np.array([(int(v) << 64) % q for v in a[i]], dtype=np.uint64)
+                         for i, (q, _) in enumerate(self.moduli)])
+
+
+def primes64(logN: int, count: int, start: int):
+    """Ascending primes q >= start, q == 1 mod 2N, q < 2^62, each with its
+    smallest quadratic non-residue (Miller-Rabin with the first 12 primes as
+    bases: deterministic below 3.3e24)."""
+    def is_prime(n):
+        if n < 2:
+            return False
+        bases = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37)
+        for p in bases:
+            if n % p == 0:
+                return n == p
+        d, s = n - 1, 0
+        while d % 2 == 0:
+            d //= 2
+            s += 1
+        for a in bases:
+            x = pow(a, d, n)
+            if x in (1, n - 1):
+                continue
+            for _ in range(s - 1):
+                x = x * x % n
+                if x == n - 1:
+                    break
+            else:
+                return False
+        return True
+    step = 2 << logN
+    q = ((max(start, 2) - 2) // step + 1) * step + 1
+    out = []
+    while len(out) < count:
+        if is_prime(q):
+            g = 2
+            while pow(g, (q - 1) // 2, q) != q - 1:
+                g += 1
+            out.append((q, g))
+        q += step
+    return out

@@ -18,7 +18,7 @@ def declared_symbols():
     for fn in os.listdir(INCLUDE):
         if fn.endswith(".h"):
             src = open(os.path.join(INCLUDE, fn)).read()
-            names |= set(re.findall(r"^NTT_API [^(]*?\b(ntt_\w+)\(", src, re.M))
+            names |= set(re.findall(r"^NTT_API [^(]*?\b(ntt\w+)\(", src, re.M))
     return sorted(names)
 
 
@@ -176,3 +176,29 @@ def test_server_and_batch_without_device_fail_cleanly():
         nb.Server(streams=-1)
     assert e.value.name == "NTT_ERR_INVALID_ARGUMENT"
     assert nb.tables_device_bytes() == 0
+
+
+@pytest.mark.parametrize("logN,count,start", [(12, 3, 1 << 59), (16, 4, 1 << 60), (17, 2, 3 << 60)])
+def test_find_moduli64_matches_oracle(logN, count, start):
+    got = [tuple(m) for m in nb.find_moduli64(logN, count, start)]
+    assert got == O.primes64(logN, count, start)
+    for q, g in got:
+        assert q < 1 << 62 and (q - 1) % (2 << logN) == 0
+
+
+def test_plan64_validation_without_device():
+    import torch
+    mods = O.primes64(12, 1, 1 << 59)
+    cases = [([(mods[0][0] + 2, 3)], "NTT_ERR_MODULUS"),          # not 1 mod 2N
+             ([((1 << 62) + (2 << 12) + 1, 3)], None),             # >= 2^62 (and maybe not 1 mod 2N)
+             ([(mods[0][0], 1)], "NTT_ERR_ROOT")]                  # 1 is a residue
+    for m, want in cases:
+        with pytest.raises(nb.NttError) as e:
+            nb.Plan64(12, m)
+        if want:
+            assert e.value.name == want
+        elif torch.cuda.is_available():
+            assert e.value.name in ("NTT_ERR_MODULUS", "NTT_ERR_MODULUS_RANGE")
+    with pytest.raises(nb.NttError) as e:
+        nb.Plan64(18, mods)
+    assert e.value.name == "NTT_ERR_UNSUPPORTED"

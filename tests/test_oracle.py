@@ -115,3 +115,17 @@ def test_oracle_against_reference_harness():
         R.ref_cpu_transform_limbs(O._ptr(ref2), logN, 3, O._ptr(T.q), O._ptr(T.inv_tab),
                                   O._ptr(T.degree_inv), 3)
         assert np.array_equal(ref2, T.inverse(ref))
+
+
+@pytest.mark.parametrize("logN", [1, 4, 9])
+def test_oracle64_matches_definition_and_roundtrips(logN):
+    """The 64-bit restatement (CT / GS loops with 128-bit products) equals the
+    O(N^2) evaluation of the bit-reversed negacyclic transform, and the
+    inverse undoes it."""
+    mods = O.primes64(logN, 3, (1 << 61) + 12345)
+    T = O.LimbTables64(logN, mods)
+    rng = np.random.default_rng(logN)
+    x = np.stack([rng.integers(0, int(q), 1 << logN, dtype=np.uint64) for q in T.q])
+    f = T.forward(x)
+    assert np.array_equal(f, T.direct(x))
+    assert np.array_equal(T.inverse(f), x)
