@@ -357,6 +357,7 @@ def run_ours(args):
     alg_bytes = 8.0 * P * LIMBS * N
     fwd_avg, inv_avg = float(fwd_ms.mean()), float(inv_ms.mean())
     dom, dom_ms = ("forward", fwd_avg) if fwd_avg >= inv_avg else ("inverse", inv_avg)
+    kname = kernel_name(nb, plan.info, dom)
     achieved = alg_bytes / (dom_ms / 1000.0) / 1e9
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
@@ -397,12 +398,12 @@ def run_ours(args):
         "per_call": {"value": 2 * P * LIMBS * world / (per_call_ms / 1000.0), "unit": "limb-NTT/s",
                      "ms_per_step": per_call_ms, "launches_per_step": 2 * P,
                      "form": "one ntt_forward + one ntt_inverse call per polynomial"},
-        "roofline": {"bound": "hbm", "kernel": f"fused_kernel ({dom})", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "forward_ms": fwd_avg, "inverse_ms": inv_avg},
-        "int_roofline": {"bound": "int-multiply", "kernel": f"fused_kernel ({dom})",
+        "int_roofline": {"bound": "int-multiply", "kernel": kname,
                          "achieved": int_achieved / 1e12, "peak": int_peak / 1e12,
                          "unit": "T mul/s", "frac": int_achieved / int_peak,
                          "peak_source": "measured (ntt_measure_int_peak: Shoup mul.hi + "
@@ -547,13 +548,26 @@ def bench_batched(args, torch, nb, stream):
     return res
 
 
+def kernel_name(nb, info, direction):
+    """The kernel template a plan launches for one direction, as the launch
+    list names it: split_kernel (phases meeting in place through L2) or
+    fused_kernel (phases meeting in the cluster's shared memory)."""
+    idx = info.fwd_config if direction == "forward" else info.inv_config
+    c = nb.kernel_configs()[idx]
+    if c.exchange == 1:
+        return (f"split_kernel<SplitGeo<{c.logN}, {c.cluster_ctas.bit_length() - 1}, "
+                f"{c.words_log2}, {c.k2a}, {c.k2b}>> ({direction})")
+    return (f"fused_kernel ({direction}; {c.cluster_ctas} CTAs, r1 {c.r1}, "
+            f"{1 << c.words_log2} words per thread)")
+
+
 def bench_multiply(args, torch, nb, stream):
     """Fused negacyclic multiply: 128 pairs of 2^16 x 24-limb polynomials
     (24 ascending 30-bit primes q == 1 mod 2^17 above 2^29.5), uniform [0, q)
     coefficients; c = a * b into b's buffer.  Fused: ntt_multiply_many, one
-    persistent launch over every (pair, limb) job: NTT(b), NTT(a), the
-    pointwise Montgomery product and INTT per limb, a read once and b read
-    and written once (12 bytes per coefficient).  Unfused: the plain calls
+    launch with a thread-block cluster per (pair, limb) job: NTT(b), NTT(a),
+    the pointwise Montgomery product and INTT per limb, a read once and b
+    read and written once (12 bytes per coefficient).  Unfused: the plain calls
     forward_many(a), forward_many(b), pointwise_mul, inverse_many(b) (4
     launches, 36 bytes per coefficient; a is overwritten by its spectrum,
     which favours it).  Batch tiles: the same products as multiply tiles of
@@ -608,7 +622,8 @@ def bench_multiply(args, torch, nb, stream):
         "value": products / (fused_ms / 1000.0), "unit": "limb-products/s",
         "limb_ntt_per_s": 3 * products / (fused_ms / 1000.0),
         "ms_per_step": fused_ms, "launches_per_step": 1,
-        "form": "ntt_multiply_many: one persistent launch (NTT(b), NTT(a), product, INTT per limb)",
+        "form": "ntt_multiply_many: one launch, a cluster per (pair, limb): NTT(b), NTT(a), "
+                "product, INTT",
         "algorithmic_bytes": 12 * words,
         "achieved_gbs": 12 * words / (fused_ms / 1000.0) / 1e9,
         "unfused": {"value": products / (unfused_ms / 1000.0), "ms_per_step": unfused_ms,
