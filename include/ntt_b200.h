@@ -213,10 +213,17 @@ NTT_API ntt_status_t ntt_measure_int_peak(double* muls_per_second);
  * caller-owned device buffers, the reference's Montgomery-form tables
  * (twiddle_dev[limb*N + i] = to_mont(psi^bitrev(i))), launched on the legacy
  * default stream.  phase1/phase2: the LC's NTT (or INTT) phase triples, or
- * NULL for DefaultNTTLaunchConfig<logN>.  On first use of a given set of
- * table pointers the tables are converted once on the device into Shoup form
- * and cached (so the caller's tables must stay unchanged while in use; see
- * ntt_shim_cache_clear).  Unlike the reference, errors are returned. */
+ * NULL for DefaultNTTLaunchConfig<logN>.  The reference's kernels read these
+ * tables at every launch; here each call first runs a refresh kernel on the
+ * same stream that compares the caller's table words and per-limb moduli,
+ * q_inv and r2 / degree_inv against shadow copies on the device and re-derives
+ * the Shoup-form entries that changed, then the transform: a caller that
+ * rewrites its tables in place (new moduli at the same addresses) gets the new
+ * results, with no host synchronisation.  The first call with a given set of
+ * pointers allocates the converted table and its shadows (cudaMalloc); later
+ * calls allocate nothing.  Unlike the reference, errors are returned; a
+ * modulus the refresh finds even or not below 2^31 is reported by
+ * ntt_shim_check. */
 NTT_API ntt_status_t ntt_launch_ntt(uint32_t* A_dev, const uint32_t* twiddle_dev,
                             const uint32_t* moduli_dev, const uint32_t* q_inv_dev,
                             const uint32_t* r2_dev, size_t limb_count, int logN,
@@ -225,8 +232,12 @@ NTT_API ntt_status_t ntt_launch_intt(uint32_t* A_dev, const uint32_t* inv_twiddl
                              const uint32_t* moduli_dev, const uint32_t* q_inv_dev,
                              const uint32_t* degree_inv_dev, size_t limb_count, int logN,
                              const PhaseConfig* phase1, const PhaseConfig* phase2);
-/* Frees the converted tables cached by the drop-in launchers. */
+/* Frees the converted tables and shadows kept by the drop-in launchers. */
 NTT_API void ntt_shim_cache_clear(void);
+/* Synchronises and reports NTT_ERR_MODULUS_RANGE if a drop-in call since the
+ * last check named a modulus that is even or not below 2^31 (the reference's
+ * Montgomery range); clears the record. */
+NTT_API ntt_status_t ntt_shim_check(void);
 
 #ifdef __cplusplus
 }

@@ -155,6 +155,7 @@ _sig("ntt_launch_ntt", _st, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_i
 _sig("ntt_launch_intt", _st, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_int,
      ctypes.POINTER(PhaseConfig), ctypes.POINTER(PhaseConfig))
 _sig("ntt_shim_cache_clear", None)
+_sig("ntt_shim_check", _st)
 _sig("ntt_config_count", ctypes.c_int)
 _sig("ntt_config_get", _st, ctypes.c_int, ctypes.POINTER(KernelConfig))
 _sig("ntt_autotune", _st, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -405,6 +406,12 @@ def launch_intt(A_dev, inv_twiddle_dev, moduli_dev, q_inv_dev, degree_inv_dev, l
 
 def shim_cache_clear():
     _lib.ntt_shim_cache_clear()
+
+
+def shim_check():
+    """Raises NTT_ERR_MODULUS_RANGE if a drop-in call since the last check
+    named a modulus that is even or not below 2^31 (synchronises)."""
+    _check(_lib.ntt_shim_check(), "ntt_shim_check")
 
 
 def measure_int_peak() -> float:

@@ -846,8 +846,8 @@ struct ShimKey {
 };
 std::mutex g_shim_mu;
 struct ShimTable {
-    TwPair* table;
-    bool lazy2;  // some modulus >= 2^30
+    TwPair* table;     // converted (Shoup) entries, tw_slot order
+    uint32_t* shadow;  // source words and limb parameters they came from
 };
 std::map<ShimKey, ShimTable> g_shim;
 
@@ -858,42 +858,53 @@ ntt_status_t shim_run(uint32_t* A, const uint32_t* tw, const uint32_t* moduli, c
         return fail(NTT_ERR_INVALID_ARGUMENT, "NULL device pointer");
     if (logN < NTT_MIN_LOGN || logN > NTT_MAX_LOGN) return fail(NTT_ERR_UNSUPPORTED, "logN %d", logN);
     if (limbs == 0) return NTT_OK;
-    if (limbs > (1u << 20)) return fail(NTT_ERR_INVALID_ARGUMENT, "limb_count too large");
+    if (limbs > 65535) return fail(NTT_ERR_INVALID_ARGUMENT, "limb_count above 65535");
     if (ph1 && ph2 && ph1->radix_stages + ph2->radix_stages != logN)
         return fail(NTT_ERR_INVALID_ARGUMENT, "phase radix_stages must add up to logN");
     int dev = 0;
     NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
     ShimKey k{dev, tw, moduli, qinv, aux, limbs, logN, inverse ? 1 : 0};
-    TwPair* table = nullptr;
-    bool lazy2 = false;
+    const size_t N = size_t{1} << logN;
+    ShimTable st{nullptr, nullptr};
     {
         std::lock_guard<std::mutex> lk(g_shim_mu);
         auto it = g_shim.find(k);
-        if (it != g_shim.end()) {
-            table = it->second.table;
-            lazy2 = it->second.lazy2;
-        }
+        if (it != g_shim.end()) st = it->second;
     }
-    if (!table) {
-        const size_t N = size_t{1} << logN;
-        std::vector<uint32_t> qh(limbs);
-        NTT_CUDA_TRY(cudaMemcpy(qh.data(), moduli, limbs * 4, cudaMemcpyDeviceToHost),
-                     "moduli read");
-        for (uint32_t q : qh) lazy2 |= q >= (1u << 30);
-        NTT_CUDA_TRY(cudaMalloc(&table, limbs * N * sizeof(TwPair)), "cudaMalloc(shim table)");
-        cudaError_t e = launch_twiddle_import(table, tw, moduli, qinv, aux, (int)limbs, logN,
-                                              inverse ? 1 : 0, 0);
+    if (!st.table) {
+        // first call with these pointers: allocate; the refresh below
+        // converts every entry (zeroed shadows, forced)
+        const size_t shadow_words = limbs * N + 3 * limbs + 2;
+        NTT_CUDA_TRY(cudaMalloc(&st.table, limbs * N * sizeof(TwPair)), "cudaMalloc(shim table)");
+        cudaError_t e = cudaMalloc(&st.shadow, shadow_words * 4);
+        if (e == cudaSuccess) e = cudaMemsetAsync(st.shadow, 0, shadow_words * 4, 0);
+        if (e == cudaSuccess)
+            e = launch_shim_refresh(st.table, st.shadow, tw, moduli, qinv, aux, (int)limbs, logN,
+                                    inverse ? 1 : 0, /*force=*/1, 0);
         if (e != cudaSuccess) {
-            cudaFree(table);
-            return cuda_fail(e, "twiddle import");
+            cudaFree(st.table);
+            if (st.shadow) cudaFree(st.shadow);
+            return cuda_fail(e, "shim table conversion");
         }
         std::lock_guard<std::mutex> lk(g_shim_mu);
-        auto ins = g_shim.insert({k, ShimTable{table, lazy2}});
+        auto ins = g_shim.insert({k, st});
         if (!ins.second) {  // another thread won the race
-            cudaFree(table);
-            table = ins.first->second.table;
+            cudaFree(st.table);
+            cudaFree(st.shadow);
+            st = ins.first->second;
         }
+    } else {
+        // the caller may have rewritten its tables in place since the last
+        // call: re-derive whatever changed, in stream order, no host sync
+        cudaError_t e = launch_shim_refresh(st.table, st.shadow, tw, moduli, qinv, aux,
+                                            (int)limbs, logN, inverse ? 1 : 0, 0, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "shim table refresh");
     }
+    // Lazy2 ranges (q < 2^31, the reference's own Montgomery range): the
+    // moduli live in device memory and may change between calls, so the
+    // faster q < 2^30 discipline cannot be chosen without a host read.
+    const bool lazy2 = true;
+    const TwPair* table = st.table;
     const FusedConfig* cfg = nullptr;
     if (logN > kSmallMaxLogN) {
         // column stages: NTT phase 1 / INTT phase 2 (the second triple)
@@ -928,9 +939,31 @@ void ntt_shim_cache_clear(void) {
         cudaGetDevice(&cur);
         if (cur != kv.first.dev) cudaSetDevice(kv.first.dev);
         cudaFree(kv.second.table);
+        cudaFree(kv.second.shadow);
         if (cur != kv.first.dev) cudaSetDevice(cur);
     }
     g_shim.clear();
+}
+
+ntt_status_t ntt_shim_check(void) {
+    std::lock_guard<std::mutex> lk(g_shim_mu);
+    bool bad = false;
+    for (auto& kv : g_shim) {
+        int cur = 0;
+        NTT_CUDA_TRY(cudaGetDevice(&cur), "cudaGetDevice");
+        if (cur != kv.first.dev) NTT_CUDA_TRY(cudaSetDevice(kv.first.dev), "cudaSetDevice");
+        const size_t N = size_t{1} << kv.first.logN;
+        uint32_t* status = kv.second.shadow + kv.first.limbs * N + 3 * kv.first.limbs + 1;
+        uint32_t v = 0;
+        cudaError_t e = cudaMemcpy(&v, status, 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && v) e = cudaMemset(status, 0, 4);
+        if (cur != kv.first.dev) cudaSetDevice(cur);
+        if (e != cudaSuccess) return cuda_fail(e, "shim status read");
+        bad |= v != 0;
+    }
+    return bad ? fail(NTT_ERR_MODULUS_RANGE,
+                      "a drop-in call named a modulus that is even or not below 2^31")
+               : NTT_OK;
 }
 
 }  // extern "C"

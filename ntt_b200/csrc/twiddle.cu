@@ -62,6 +62,19 @@ __global__ void twiddle_gen_kernel(TwPair* out, const TwGenLimb* limbs, int logN
 // Import the reference's Montgomery-form tables (tw_mont[i] = to_mont(w_i)).
 // Forward: fold0 = R = redc(r2), fold1 = tw_mont[1] itself (= w_1 * R).
 // Inverse: fold0 = c = redc(redc(degree_inv_mont)), fold1 = w_1 * c.
+__device__ __forceinline__ uint32_t import_entry(const uint32_t* t, uint32_t i, uint32_t q,
+                                                 uint32_t qi, uint32_t aux, int inverse) {
+    if (!inverse) {
+        if (i == 0) return dev_redc(aux, q, qi);
+        if (i == 1) return t[1] % q;
+        return dev_redc(t[i], q, qi);
+    }
+    const uint32_t c = dev_redc(dev_redc(aux, q, qi), q, qi);
+    if (i == 0) return c;
+    if (i == 1) return (uint32_t)(((uint64_t)dev_redc(t[1], q, qi) * c) % q);
+    return dev_redc(t[i], q, qi);
+}
+
 __global__ void twiddle_import_kernel(TwPair* out, const uint32_t* tw_mont,
                                       const uint32_t* moduli, const uint32_t* nqinv,
                                       const uint32_t* aux, int logN, int inverse) {
@@ -69,20 +82,63 @@ __global__ void twiddle_import_kernel(TwPair* out, const uint32_t* tw_mont,
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const uint32_t l = blockIdx.y;
-    const uint32_t q = moduli[l], qi = nqinv[l];
-    const uint32_t* t = tw_mont + (size_t)l * N;
-    uint32_t w;
-    if (!inverse) {
-        if (i == 0) w = dev_redc(aux[l], q, qi);
-        else if (i == 1) w = t[1] % q;
-        else w = dev_redc(t[i], q, qi);
-    } else {
-        const uint32_t c = dev_redc(dev_redc(aux[l], q, qi), q, qi);
-        if (i == 0) w = c;
-        else if (i == 1) w = (uint32_t)(((uint64_t)dev_redc(t[1], q, qi) * c) % q);
-        else w = dev_redc(t[i], q, qi);
-    }
+    const uint32_t q = moduli[l];
+    const uint32_t w = import_entry(tw_mont + (size_t)l * N, i, q, nqinv[l], aux[l], inverse);
     out[(size_t)l * N + tw_slot(i, logN)] = TwPair{w, (uint32_t)(((uint64_t)w << 32) / q)};
+}
+
+// Stream-ordered refresh of a converted table against the caller's
+// Montgomery-form table, once per drop-in call: entry i of limb l is
+// re-derived when its source word, or the limb's modulus, -q^{-1} or
+// auxiliary constant, differs from the shadow copy it was derived from.
+// `force` re-derives every entry (the first call).
+// Shadow layout: limbs * N source words, then (q, qinv, aux) per limb, then
+// a block counter and a status word.  Every block compares the limb
+// parameters against their shadows; the last block to finish (the counter)
+// stores the new parameters, so no block can see half-updated shadows.  A
+// modulus that is even or not below 2^31 sets status bit 0 (the converted
+// entries would be meaningless; ntt_shim_check reports it).
+__global__ void shim_refresh_kernel(TwPair* out, uint32_t* shadow, const uint32_t* tw_mont,
+                                    const uint32_t* moduli, const uint32_t* nqinv,
+                                    const uint32_t* aux, int limbs, int logN, int inverse,
+                                    int force) {
+    const uint32_t N = 1u << logN;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t l = blockIdx.y;
+    uint32_t* params = shadow + (size_t)limbs * N;
+    uint32_t* counter = params + 3 * (size_t)limbs;
+    uint32_t* status = counter + 1;
+    const uint32_t q = moduli[l], qi = nqinv[l], ax = aux[l];
+    const bool changed = force || q != params[3 * l] || qi != params[3 * l + 1] || ax != params[3 * l + 2];
+    if (i < N) {
+        const uint32_t* t = tw_mont + (size_t)l * N;
+        const uint32_t src = t[i];
+        uint32_t* sh = shadow + (size_t)l * N + i;
+        if (changed || src != *sh) {
+            if ((q & 1u) && q < (1u << 31)) {
+                const uint32_t w = import_entry(t, i, q, qi, ax, inverse);
+                out[(size_t)l * N + tw_slot(i, logN)] =
+                    TwPair{w, (uint32_t)(((uint64_t)w << 32) / q)};
+            } else if (i == 0) {
+                atomicOr(status, 1u);
+            }
+            *sh = src;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t blocks = gridDim.x * gridDim.y;
+        if (atomicAdd(counter, 1u) == blocks - 1) {
+            __threadfence();
+            for (int k = 0; k < limbs; ++k) {
+                params[3 * k] = moduli[k];
+                params[3 * k + 1] = nqinv[k];
+                params[3 * k + 2] = aux[k];
+            }
+            *counter = 0;
+        }
+    }
 }
 
 cudaError_t launch_twiddle_gen(TwPair* out, const TwGenLimb* limbs_dev, int limbs, int logN,
@@ -100,6 +156,17 @@ cudaError_t launch_twiddle_import(TwPair* out, const uint32_t* tw_mont, const ui
     dim3 block(N < 256 ? N : 256), grid((N + block.x - 1) / block.x, limbs);
     twiddle_import_kernel<<<grid, block, 0, s>>>(out, tw_mont, moduli, nqinv, aux, logN,
                                                  inverse);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shim_refresh(TwPair* out, uint32_t* shadow, const uint32_t* tw_mont,
+                                const uint32_t* moduli, const uint32_t* nqinv,
+                                const uint32_t* aux, int limbs, int logN, int inverse,
+                                int force, cudaStream_t s) {
+    const uint32_t N = 1u << logN;
+    dim3 block(N < 256 ? N : 256), grid((N + block.x - 1) / block.x, limbs);
+    shim_refresh_kernel<<<grid, block, 0, s>>>(out, shadow, tw_mont, moduli, nqinv, aux, limbs,
+                                               logN, inverse, force);
     return cudaGetLastError();
 }
 

@@ -22,5 +22,11 @@ cudaError_t launch_twiddle_gen(TwPair* out, const TwGenLimb* limbs_dev, int limb
 cudaError_t launch_twiddle_import(TwPair* out, const uint32_t* tw_mont, const uint32_t* moduli,
                                   const uint32_t* nqinv, const uint32_t* aux, int limbs,
                                   int logN, int inverse, cudaStream_t s);
+// shadow: limbs * N + 3 * limbs + 2 words, zeroed before the first (forced)
+// call.
+cudaError_t launch_shim_refresh(TwPair* out, uint32_t* shadow, const uint32_t* tw_mont,
+                                const uint32_t* moduli, const uint32_t* nqinv,
+                                const uint32_t* aux, int limbs, int logN, int inverse,
+                                int force, cudaStream_t s);
 
 }  // namespace nttb

@@ -226,6 +226,59 @@ def test_dropin_launchers_match_reference_tables(torch_cuda, nb):
     nb.shim_cache_clear()
 
 
+def test_dropin_tables_rewritten_in_place(torch_cuda, nb):
+    """A caller that rewrites its tables and moduli at the same addresses gets
+    the new moduli's results on the next call (the reference reads its tables
+    at every launch); one changed table word alone is picked up too; a
+    modulus outside the Montgomery range is reported by shim_check."""
+    torch = torch_cuda
+    logN = 13
+    mods_a, mods_b = moduli_set(logN, 4, 30), moduli_set(logN, 4, 31)
+    Ta, Tb = O.LimbTables(logN, mods_a), O.LimbTables(logN, mods_b)
+    bufs = None
+    for T in (Ta, Tb, Ta):
+        tw, itw = T.mont_tables()
+        arrays = (tw, itw, T.q, T.q_inv, T.r2, T.degree_inv_mont)
+        if bufs is None:
+            bufs = [dev(torch, a) for a in arrays]
+        else:  # same addresses, new contents
+            for b, a in zip(bufs, arrays):
+                b.copy_(dev(torch, a))
+        tw_d, itw_d, q_d, qi_d, r2_d, di_d = bufs
+        x = O.uniform_limbs(logN, T.q, 7)
+        d = dev(torch, x)
+        nb.launch_ntt(d, tw_d, q_d, qi_d, r2_d, 4, logN, None, None)
+        torch.cuda.synchronize()
+        assert np.array_equal(host(d), T.forward_mont(x, THREADS))
+        nb.launch_intt(d, itw_d, q_d, qi_d, di_d, 4, logN, None, None)
+        torch.cuda.synchronize()
+        assert np.array_equal(host(d), x)
+    nb.shim_check()
+    # one table word changed (entry 5 of limb 2 set to entry 6's value): the
+    # forward must follow the edited table, entry by entry
+    tw, _ = Ta.mont_tables()
+    tw = tw.copy()
+    tw[2, 5] = tw[2, 6]
+    bufs[0].copy_(dev(torch, tw))
+    x = O.uniform_limbs(logN, Ta.q, 8)
+    d = dev(torch, x)
+    nb.launch_ntt(d, bufs[0], bufs[2], bufs[3], bufs[4], 4, logN, None, None)
+    torch.cuda.synchronize()
+    got = host(d)
+    assert np.array_equal(got[[0, 1, 3]], Ta.forward_mont(x, THREADS)[[0, 1, 3]])
+    assert not np.array_equal(got[2], Ta.forward_mont(x, THREADS)[2])
+    # a modulus above the range: reported, not silently used
+    q_bad = Ta.q.copy()
+    q_bad[1] = (1 << 31) + 11
+    bufs[2].copy_(dev(torch, q_bad))
+    nb.launch_ntt(d, bufs[0], bufs[2], bufs[3], bufs[4], 4, logN, None, None)
+    with pytest.raises(nb.NttError) as e:
+        nb.shim_check()
+    assert e.value.name == "NTT_ERR_MODULUS_RANGE"
+    nb.shim_check()  # the record was cleared
+    nb.shim_cache_clear()
+
+
 def test_reference_v04_gpu_output(torch_cuda, nb):
     """Third reference: the reference's own launch_ntt / launch_intt, built
     unchanged for sm_100a (oracle/_ref), on the same inputs."""
