@@ -180,6 +180,44 @@ NTT_API ntt_status_t ntt_forward_scaled(const ntt_plan_t* plan, uint32_t* a_dev,
 NTT_API ntt_status_t ntt_inverse_scaled(const ntt_plan_t* plan, uint32_t* a_dev, size_t polys,
                                         size_t poly_stride, const uint32_t* scale_dev,
                                         ntt_stream_t stream);
+/* The NTT steps of RNS basis conversion (ModUp / ModDown), each one launch of
+ * the plan's transform kernels, same layout and alignment rules as
+ * ntt_forward_many; limb indices are the plan's.
+ *
+ * ntt_forward_skip (ModUp's forward; Cheddar's NTTForModUp,
+ * src/NTT_cheddar.cu:886-955): the forward of every limb except
+ * [skip_begin, skip_end), which the launch neither reads nor writes (the
+ * limbs of the decomposition digit that are already in the NTT domain).
+ *
+ * ntt_forward_sub_scale (ModDown's forward; NTTForModDown and
+ * NTTPhase2ForModDown, src/NTT_cheddar.cu:456-601, 957-1027): per limb l
+ *   a_l <- (NTT(a_l) - d_k * s_l) * c_l   (mod q_l), canonical,
+ * where s_l = sub_dev[p * sub_stride + k * N + i] with k = l - sub_begin
+ * for sub_begin <= l < sub_end (s_l = 0 for the other limbs), in the
+ * forward's output domain (Montgomery); c_l = scale_dev[l] (NULL: 1) and
+ * d_k = sub_mul_dev[k] (NULL: 1, Cheddar's src2_padding) are normal-domain
+ * constants.  c enters through stage 0 as in ntt_forward_scaled and the
+ * subtraction of (c d) s rides on the final store, so HBM sees a read and
+ * written once and s read once.  sub_stride 0 = packed (sub_end - sub_begin)
+ * * N; sub_dev 16-byte aligned for logN >= 10 and must not overlap a_dev.
+ *
+ * ntt_inverse_scaled_range (INTTForModDown / INTTAndMultConst on part of the
+ * basis, src/NTT_cheddar.cu:743-813, 1029-1128): a_l <- c_k * INTT(a_l) for
+ * the limbs l in [limb_begin, limb_end) only, c_k = scale_dev[l -
+ * limb_begin] (NULL: 1); the reference writes a separate buffer, this one
+ * transforms in place. */
+NTT_API ntt_status_t ntt_forward_skip(const ntt_plan_t* plan, uint32_t* a_dev, size_t polys,
+                                      size_t poly_stride, int skip_begin, int skip_end,
+                                      ntt_stream_t stream);
+NTT_API ntt_status_t ntt_forward_sub_scale(const ntt_plan_t* plan, uint32_t* a_dev, size_t polys,
+                                           size_t poly_stride, const uint32_t* sub_dev,
+                                           size_t sub_stride, int sub_begin, int sub_end,
+                                           const uint32_t* scale_dev, const uint32_t* sub_mul_dev,
+                                           ntt_stream_t stream);
+NTT_API ntt_status_t ntt_inverse_scaled_range(const ntt_plan_t* plan, uint32_t* a_dev,
+                                              size_t polys, size_t poly_stride, int limb_begin,
+                                              int limb_end, const uint32_t* scale_dev,
+                                              ntt_stream_t stream);
 /* c = a (.) b: pointwise Montgomery product of two forward outputs (x*2^32
  * domain) per limb modulus, giving the spectrum of the negacyclic product
  * for ntt_inverse.  Over `polys` polynomials (poly_stride words apart, 0 =

@@ -171,6 +171,12 @@ _sig("ntt_autotune_reload", None)
 _sig("ntt_selftest_wait_expiry", _st, _vp, ctypes.c_uint32, _vp)
 _sig("ntt_forward_scaled", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp, _vp)
 _sig("ntt_inverse_scaled", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp, _vp)
+_sig("ntt_forward_skip", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int,
+     ctypes.c_int, _vp)
+_sig("ntt_forward_sub_scale", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp,
+     ctypes.c_size_t, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp)
+_sig("ntt_inverse_scaled_range", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int,
+     ctypes.c_int, _vp, _vp)
 
 
 def _check(st: int, where: str):
@@ -361,6 +367,32 @@ class Plan:
         """a <- c_l * INTT(a) per limb l (see forward_scaled)."""
         _check(_lib.ntt_inverse_scaled(self._h, _ptr(a), polys, poly_stride, _ptr(scale),
                                        _stream(stream)), "ntt_inverse_scaled")
+
+    def forward_skip(self, a, skip_begin: int, skip_end: int, polys: int = 1,
+                     poly_stride: int = 0, stream=None):
+        """ModUp's forward: every limb except [skip_begin, skip_end)."""
+        _check(_lib.ntt_forward_skip(self._h, _ptr(a), polys, poly_stride, skip_begin, skip_end,
+                                     _stream(stream)), "ntt_forward_skip")
+
+    def forward_sub_scale(self, a, sub, sub_begin: int, sub_end: int, scale=None, sub_mul=None,
+                          polys: int = 1, poly_stride: int = 0, sub_stride: int = 0,
+                          stream=None):
+        """ModDown's forward: a_l <- (NTT(a_l) - d_k s_l) c_l per limb l, s_l
+        the limb k = l - sub_begin of `sub` for l in [sub_begin, sub_end)
+        (0 elsewhere); `scale` (c) and `sub_mul` (d): optional device arrays of
+        normal-domain constants, per plan limb and per sub limb."""
+        _check(_lib.ntt_forward_sub_scale(self._h, _ptr(a), polys, poly_stride, _ptr(sub),
+                                          sub_stride, sub_begin, sub_end, _ptr(scale),
+                                          _ptr(sub_mul), _stream(stream)),
+               "ntt_forward_sub_scale")
+
+    def inverse_scaled_range(self, a, limb_begin: int, limb_end: int, scale=None,
+                             polys: int = 1, poly_stride: int = 0, stream=None):
+        """a_l <- c_k INTT(a_l) for limbs l in [limb_begin, limb_end) only,
+        c_k = scale[l - limb_begin] (None: 1)."""
+        _check(_lib.ntt_inverse_scaled_range(self._h, _ptr(a), polys, poly_stride, limb_begin,
+                                             limb_end, _ptr(scale), _stream(stream)),
+               "ntt_inverse_scaled_range")
 
     def pointwise_mul(self, c, a, b, polys: int = 1, poly_stride: int = 0, stream=None):
         """c = a (.) b: Montgomery product of two forward outputs per limb."""

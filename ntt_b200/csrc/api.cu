@@ -178,8 +178,9 @@ static uint32_t smem_of(const FusedConfig* c, int schedule) {
 }
 
 static const void* kernel_of(const FusedConfig* c, bool fwd, int schedule, bool lazy2,
-                             bool mul = false) {
+                             bool mul = false, bool sub = false) {
     if (mul) return c->kern_mul[lazy2 ? 1 : 0];
+    if (sub) return c->kern_sub[lazy2 ? 1 : 0];
     return c->kernel(schedule == NTT_SCHEDULE_STAGED, fwd, lazy2);
 }
 
@@ -251,11 +252,11 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule) {
 // wave of resident clusters, each running a contiguous chunk of limb-major
 // jobs with the next input slab bulk-copied ahead.
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
-                          int schedule, bool lazy2, bool mul) {
+                          int schedule, bool lazy2, bool mul, bool sub) {
     if (a.jobs == 0) return NTT_OK;
-    // the product epilogue and the split kernels have a direct form only
-    if (mul || c->split) schedule = NTT_SCHEDULE_DIRECT;
-    const void* fn = kernel_of(c, fwd, schedule, lazy2, mul);
+    // the output epilogues and the split kernels have a direct form only
+    if (mul || sub || c->split) schedule = NTT_SCHEDULE_DIRECT;
+    const void* fn = kernel_of(c, fwd, schedule, lazy2, mul, sub);
     ntt_status_t st = prepare_function(c, fn, schedule);
     if (st != NTT_OK) return st;
     const unsigned C = 1u << c->clog;
@@ -644,9 +645,18 @@ namespace nttb {
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
                            cudaStream_t s, uint32_t* status, int schedule, bool lazy2,
-                           const uint32_t* mul_src, const uint32_t* scale) {
-    if (polys == 0) return NTT_OK;
+                           const uint32_t* mul_src, const uint32_t* scale, const LimbOps* ops) {
+    static const LimbOps kNone{};
+    if (!ops) ops = &kNone;
+    const bool sub = ops->sub != nullptr;
+    if (polys == 0 || limbs == 0) return NTT_OK;
     if (!a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL data pointer");
+    if (sub && (!fwd || mul_src))
+        return fail(NTT_ERR_UNSUPPORTED, "the subtract-and-scale output follows a plain forward");
+    if (sub && cfg && ((((uintptr_t)ops->sub & 15u) != 0) || (polys > 1 && (ops->sub_stride & 3u) != 0)))
+        return fail(NTT_ERR_MISALIGNED, "sub must be 16-byte aligned (sub_stride a multiple of 4 words)");
+    if (sub && ((uintptr_t)ops->sub & 3u) != 0)
+        return fail(NTT_ERR_MISALIGNED, "sub must be 4-byte aligned");
     if (mul_src && (!cfg || !fwd))
         return fail(NTT_ERR_UNSUPPORTED, "the product epilogue needs a fused forward (logN >= 10)");
     // split configurations transform in place through the data buffer, which
@@ -672,17 +682,21 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
     if (cfg) {
         FusedArgs fa{a,  tw, q, (uint32_t)limbs, (uint32_t)polys, (uint32_t)jobs, 1u,
                      (unsigned long long)stride, status, mul_src, (unsigned long long)stride,
-                     scale};
-        return launch_fused(cfg, fwd, fa, s, schedule, lazy2, mul_src != nullptr);
+                     scale, ops->skip_at, ops->skip_len, ops->sub,
+                     (unsigned long long)ops->sub_stride, ops->sub_begin, ops->sub_end,
+                     ops->sub_mul};
+        return launch_fused(cfg, fwd, fa, s, schedule, lazy2, mul_src != nullptr, sub);
     }
     SmallArgs sa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride, logN,
-                 scale};
+                 scale, ops->skip_at, ops->skip_len, ops->sub,
+                 (unsigned long long)ops->sub_stride, ops->sub_begin, ops->sub_end, ops->sub_mul};
     NTT_CUDA_TRY(launch_small(sa, fwd, s), "small NTT launch");
     return NTT_OK;
 }
 
 static ntt_status_t plan_run(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
-                             bool fwd, ntt_stream_t s, const uint32_t* scale = nullptr) {
+                             bool fwd, ntt_stream_t s, const uint32_t* scale = nullptr,
+                             const LimbOps* ops = nullptr, int limb_begin = 0, int limb_end = -1) {
     if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
     int dev = 0;
     NTT_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
@@ -692,9 +706,20 @@ static ntt_status_t plan_run(const ntt_plan_t* p, uint32_t* a, size_t polys, siz
     if (stride == 0) stride = (size_t)p->limbs << p->logN;
     const FusedConfig* cfg = fwd ? p->cfg_fwd : p->cfg_inv;
     if (cfg && (polys == 1 || polys < (size_t)cfg->np)) cfg = fwd ? p->cfg_fwd1 : p->cfg_inv1;
-    return run_transform(p->logN, cfg, fwd ? p->fwd : p->inv, p->q,
-                         p->limbs, a, polys, stride, fwd, (cudaStream_t)s, p->status,
-                         p->schedule, p->lazy2, nullptr, scale);
+    // a limb range [limb_begin, limb_end) runs as a plan over those limbs:
+    // tables, moduli and data offset by limb_begin limbs, same stride
+    if (limb_end < 0) limb_end = p->limbs;
+    const size_t off = (size_t)limb_begin << p->logN;
+    int launch_limbs = limb_end - limb_begin;
+    if (ops) launch_limbs -= (int)ops->skip_len;
+    return run_transform(p->logN, cfg, (fwd ? p->fwd : p->inv) + off, p->q + limb_begin,
+                         launch_limbs, a ? a + off : nullptr, polys, stride, fwd,
+                         (cudaStream_t)s, p->status, p->schedule, p->lazy2, nullptr, scale, ops);
+}
+
+// The extent in words of `polys` polynomials of `limbs` limbs `stride` apart.
+static size_t extent_words(size_t polys, size_t stride, size_t limbs, int logN) {
+    return (polys - 1) * stride + (limbs << logN);
 }
 
 }  // namespace nttb
@@ -725,6 +750,60 @@ ntt_status_t ntt_inverse_scaled(const ntt_plan_t* p, uint32_t* a, size_t polys, 
                                 const uint32_t* scale, ntt_stream_t s) {
     if (!scale) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL scale array");
     return plan_run(p, a, polys, stride, false, s, scale);
+}
+
+ntt_status_t ntt_forward_skip(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
+                              int skip_begin, int skip_end, ntt_stream_t s) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    if (skip_begin < 0 || skip_end < skip_begin || skip_end > p->limbs)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "skip range [%d, %d) outside the plan's %d limbs",
+                    skip_begin, skip_end, p->limbs);
+    LimbOps ops;
+    ops.skip_at = (uint32_t)skip_begin;
+    ops.skip_len = (uint32_t)(skip_end - skip_begin);
+    return plan_run(p, a, polys, stride, true, s, nullptr, &ops);
+}
+
+ntt_status_t ntt_forward_sub_scale(const ntt_plan_t* p, uint32_t* a, size_t polys, size_t stride,
+                                   const uint32_t* sub, size_t sub_stride, int sub_begin,
+                                   int sub_end, const uint32_t* scale, const uint32_t* sub_mul,
+                                   ntt_stream_t s) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    if (sub_begin < 0 || sub_end < sub_begin || sub_end > p->limbs)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "sub range [%d, %d) outside the plan's %d limbs",
+                    sub_begin, sub_end, p->limbs);
+    const size_t sub_limbs = (size_t)(sub_end - sub_begin);
+    if (sub_limbs > 0 && !sub) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL sub with a non-empty range");
+    if (stride == 0) stride = (size_t)p->limbs << p->logN;
+    if (sub_stride == 0) sub_stride = sub_limbs << p->logN;
+    if (polys > 1 && sub_stride < (sub_limbs << p->logN))
+        return fail(NTT_ERR_INVALID_ARGUMENT, "sub_stride smaller than (sub_end - sub_begin) * N");
+    if (polys > 0 && sub_limbs > 0 && a) {
+        // the subtrahend is read after the transform rewrote its own buffer
+        // in place: the two must not overlap
+        const uintptr_t a0 = (uintptr_t)a, s0 = (uintptr_t)sub;
+        const uintptr_t a1 = a0 + 4 * extent_words(polys, stride, p->limbs, p->logN);
+        const uintptr_t s1 = s0 + 4 * extent_words(polys, sub_stride, sub_limbs, p->logN);
+        if (a0 < s1 && s0 < a1) return fail(NTT_ERR_INVALID_ARGUMENT, "sub overlaps the data");
+    }
+    LimbOps ops;
+    ops.sub = sub_limbs > 0 ? sub : nullptr;
+    ops.sub_stride = sub_stride;
+    ops.sub_begin = (uint32_t)sub_begin;
+    ops.sub_end = (uint32_t)sub_end;
+    ops.sub_mul = sub_mul;
+    // with an empty range the output is NTT(c x): the scaled forward
+    return plan_run(p, a, polys, stride, true, s, scale, ops.sub ? &ops : nullptr);
+}
+
+ntt_status_t ntt_inverse_scaled_range(const ntt_plan_t* p, uint32_t* a, size_t polys,
+                                      size_t stride, int limb_begin, int limb_end,
+                                      const uint32_t* scale, ntt_stream_t s) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    if (limb_begin < 0 || limb_end < limb_begin || limb_end > p->limbs)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "limb range [%d, %d) outside the plan's %d limbs",
+                    limb_begin, limb_end, p->limbs);
+    return plan_run(p, a, polys, stride, false, s, scale, nullptr, limb_begin, limb_end);
 }
 
 ntt_status_t ntt_pointwise_mul(const ntt_plan_t* p, uint32_t* c, const uint32_t* a,

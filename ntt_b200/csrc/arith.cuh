@@ -57,6 +57,13 @@ struct TwPair {
     uint32_t wp;
 };
 
+// ModDown's output word: y - e * s (mod q), canonical; y and s in [0, q),
+// e with its Shoup companion.
+NTT_HD uint32_t sub_scaled(uint32_t y, uint32_t s, TwPair e, uint32_t q) {
+    const uint32_t u = csub(shoup_mul(s, e.w, e.wp, q), q);
+    return y - u + (y < u ? q : 0u);
+}
+
 // Device twiddle-table layout of one limb (N = 2^logN entries).  In the last
 // stages every thread of the transform kernels owns a run of consecutive
 // entries (16, 8, 4, 2 of them in the last four stages with the usual 5-word
@@ -83,6 +90,28 @@ NTT_HD constexpr uint32_t tw_slot(uint32_t i, int logN) {
     }
     return i;
 }
+
+// Compressed tables (plans created with NTT_PLAN_COMPRESSED_TWIDDLES, logN >=
+// kTwCompMinLogN): per limb 3N/16 + 16 pairs instead of N.
+//   slots [0, N/16):  entries 0 .. N/16 - 1, as in the full table (stages
+//                     0 .. logN-5, folded entries 0 and 1 included);
+//   for p = 3, 2, 1, 0, at tw_comp_base(logN, p): the base block of stage
+//                     logN-1-p (H = N/2^(p+1), F = 16/2^p), B_p[m] =
+//                     tw[H + m F] for m < N/32;
+//   at tw_comp_lsb(logN): L[c] = psi^bitrev(c) (inverse psi^-bitrev(c)) for
+//                     c < 16, L[0] = 1 (never folded).
+// With j = m F + c, c < F, the bits of H + m F and of c are disjoint, so
+// bitrev(H + j) = bitrev(H + m F) + bitrev(c) and tw[H + j] = B_p[m] L[c]:
+// a butterfly of those stages multiplies by the two factors in turn (two
+// Shoup products, one when c = 0).  The base blocks are the c = 0 slots of
+// the full table's interleaved blocks, so a warp's loads stay as coalesced;
+// the factors L are the same 16 pairs for every thread (broadcast loads).
+constexpr int kTwCompMinLogN = 15;
+NTT_HD constexpr uint32_t tw_comp_base(int logN, int p) {
+    return (1u << (logN - 4)) + (uint32_t)(3 - p) * (1u << (logN - 5));
+}
+NTT_HD constexpr uint32_t tw_comp_lsb(int logN) { return 3u << (logN - 4); }
+NTT_HD constexpr uint32_t tw_comp_entries(int logN) { return tw_comp_lsb(logN) + 16u; }
 
 // ---- butterflies ----------------------------------------------------------
 
@@ -126,6 +155,19 @@ struct Lazy4 {  // q < 2^30
         x = csub(shoup_mul(s, c.w, c.wp, q), q);
         y = csub(shoup_mul(d, wc.w, wc.wp, q), q);
     }
+    // The same butterflies with the twiddle given as two factors a * b
+    // (compressed tables); Shoup products accept any 32-bit input, so the
+    // ranges are those of ct / gs.
+    NTT_HD static void ct2(uint32_t& x, uint32_t& y, TwPair a, TwPair b, uint32_t q,
+                           uint32_t q2) {
+        y = shoup_mul(y, b.w, b.wp, q);
+        ct(x, y, a.w, a.wp, q, q2);
+    }
+    NTT_HD static void gs2(uint32_t& x, uint32_t& y, TwPair a, TwPair b, uint32_t q,
+                           uint32_t q2) {
+        gs(x, y, a.w, a.wp, q, q2);
+        y = shoup_mul(y, b.w, b.wp, q);
+    }
 };
 
 struct Lazy2 {  // q < 2^31
@@ -160,6 +202,16 @@ struct Lazy2 {  // q < 2^31
         uint32_t d = x - y + q;
         x = csub(shoup_mul(s, c.w, c.wp, q), q);
         y = csub(shoup_mul(d, wc.w, wc.wp, q), q);
+    }
+    NTT_HD static void ct2(uint32_t& x, uint32_t& y, TwPair a, TwPair b, uint32_t q,
+                           uint32_t q2) {
+        y = shoup_mul(y, b.w, b.wp, q);
+        ct(x, y, a.w, a.wp, q, q2);
+    }
+    NTT_HD static void gs2(uint32_t& x, uint32_t& y, TwPair a, TwPair b, uint32_t q,
+                           uint32_t q2) {
+        gs(x, y, a.w, a.wp, q, q2);
+        y = csub(shoup_mul(y, b.w, b.wp, q), q);
     }
 };
 

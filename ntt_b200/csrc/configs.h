@@ -65,6 +65,9 @@ struct FusedConfig {
     // and its dynamic shared memory (work buffer + the spectrum of b)
     const void* kern_smul[2];
     uint32_t smem_smul;
+    // the direct forward with the subtract-and-scale output (ModDown;
+    // FusedArgs.sub): [lazy2]
+    const void* kern_sub[2];
     bool has_mul() const { return kern_mul[0] != nullptr; }
     const void* kernel(bool staged, bool fwd, bool lazy2) const {
         return kern[staged ? 1 : 0][fwd ? 1 : 0][lazy2 ? 1 : 0];

@@ -35,6 +35,45 @@ struct FusedArgs {
     // optional per-limb constants c (normal domain): the forward transforms
     // c * x, the inverse returns c * INTT(x), both folded into stage 0
     const uint32_t* scale;
+    // limb map: launch limb l is the table's limb l, or l + skip_len from
+    // skip_at on (ModUp's forward leaves the limbs already in the NTT
+    // domain alone).  Zero-initialised = the identity.
+    uint32_t skip_at, skip_len;
+    // subtract-and-scale output (forward kernels with the Sub epilogue):
+    // limb l in [sub_begin, sub_end) stores y - e_l * s, s the word at the
+    // output's place in sub[poly * sub_stride + (l - sub_begin) * N], e_l =
+    // c_l * d_{l - sub_begin} (c = scale or 1, d = sub_mul or 1); the other
+    // limbs store y.  y = NTT(c * x), so the limb stores (NTT(x) - d s) c.
+    const uint32_t* sub;
+    unsigned long long sub_stride;
+    uint32_t sub_begin, sub_end;
+    const uint32_t* sub_mul;
+};
+
+__device__ __forceinline__ uint32_t map_limb(const FusedArgs& a, uint32_t l) {
+    return l >= a.skip_at ? l + a.skip_len : l;
+}
+
+// The job's subtrahend base (nullptr when its limb has none) and constant
+// e = c * d with its Shoup companion.
+struct SubJob {
+    const uint32_t* base;
+    TwPair e;
+};
+template <int LOGN>
+__device__ __forceinline__ SubJob sub_job(const FusedArgs& a, uint32_t limb, size_t poly,
+                                          uint32_t q) {
+    if (limb < a.sub_begin || limb >= a.sub_end) return SubJob{nullptr, TwPair{0u, 0u}};
+    const uint32_t k = limb - a.sub_begin;
+    unsigned long long e = a.scale ? __ldg(a.scale + limb) % q : 1ull;
+    if (a.sub_mul) e = e * (__ldg(a.sub_mul + k) % q) % q;
+    return SubJob{a.sub + poly * a.sub_stride + ((size_t)k << LOGN),
+                  TwPair{(uint32_t)e, (uint32_t)((e << 32) / q)}};
+}
+
+struct SubOut {
+    uint32_t* p;
+    const uint32_t* s;  // nullptr: plain store
 };
 
 // The constant table entry t times c, with its Shoup companion (computed
@@ -130,11 +169,14 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst_sa, const void* src, uint3
 // Memory interface used by the pass code (ntt_core.cuh): every access is a
 // per-thread base plus a compile-time offset, which the compiler turns into
 // an immediate address offset.
-template <int C, bool Staged, int NP, bool Mul = false>
+template <int C, bool Staged, int NP, bool Mul = false, bool Sub = false>
 struct DevCtx {
     static constexpr bool kStaged = Staged;
+    static constexpr bool kSub = Sub;
     uint32_t* g[NP];  // limb base of each polynomial of the job (input)
     uint32_t* o[NP];  // ... output (the input's place, or the spectrum for Mul)
+    const uint32_t* sb[NP];  // Sub: the subtrahend's limb base (nullptr: none)
+    TwPair sub_e;            // Sub: e and its Shoup companion
     uint32_t qinv;    // Mul: -q^{-1} mod 2^32
     uint32_t live;    // Mul: bit p set when slot p is not a repeated polynomial
     const TwPair* __restrict__ twp;
@@ -162,7 +204,24 @@ struct DevCtx {
     // word at the output's place (written by an earlier launch: read via L2)
     __device__ __forceinline__ auto o_base(int p, uint32_t off) const {
         if constexpr (Mul) return MulOut{o[p] + off, ((live >> p) & 1u) != 0};
+        else if constexpr (Sub) return SubOut{o[p] + off, sb[p] ? sb[p] + off : nullptr};
         else return o[p] + off;
+    }
+    // Sub: y - e * s with the subtrahend word at the output's place (read
+    // once: streamed)
+    __device__ __forceinline__ void o_st(SubOut b, uint32_t c, uint32_t v) const {
+        b.p[c] = b.s ? sub_scaled(v, __ldcs(b.s + c), sub_e, q) : v;
+    }
+    __device__ __forceinline__ void o_st4(SubOut b, uint32_t c, uint32_t x, uint32_t y,
+                                          uint32_t z, uint32_t w) const {
+        if (b.s) {
+            const uint4 k = __ldcs(reinterpret_cast<const uint4*>(b.s + c));
+            x = sub_scaled(x, k.x, sub_e, q);
+            y = sub_scaled(y, k.y, sub_e, q);
+            z = sub_scaled(z, k.z, sub_e, q);
+            w = sub_scaled(w, k.w, sub_e, q);
+        }
+        *reinterpret_cast<uint4*>(b.p + c) = make_uint4(x, y, z, w);
     }
     __device__ __forceinline__ void o_st(uint32_t* b, uint32_t c, uint32_t v) const { b[c] = v; }
     __device__ __forceinline__ void o_st4(uint32_t* b, uint32_t c, uint32_t x, uint32_t y,
@@ -292,7 +351,8 @@ __device__ __forceinline__ void pass_sync() {
 template <class G, bool Fwd>
 __device__ __forceinline__ void issue_slab(const FusedArgs& a, uint32_t job, uint32_t rank,
                                            uint32_t stage_sa, uint32_t mbar_sa) {
-    const uint32_t limb = job / a.polys, poly = job - limb * a.polys;
+    const uint32_t jl = job / a.polys, poly = job - jl * a.polys;
+    const uint32_t limb = map_limb(a, jl);
     const uint32_t* src = a.data + (size_t)poly * a.poly_stride + ((size_t)limb << G::LOGN);
     fence_proxy_async_smem();
     if (threadIdx.x == 0) mbar_arrive_expect_tx(mbar_sa, G::M * 4u);
@@ -353,9 +413,11 @@ __device__ __forceinline__ void fused_inverse_body(Ctx& ctx, Pre&& prefetch) {
 // moduli below 2^30; Lazy2 takes any below 2^31), fixed per kernel so that
 // one path's registers fit the launch bounds.
 // Mul (forward, direct only): the product epilogue of FusedArgs.
-template <class G, bool Fwd, bool Staged, class Arith, bool Mul = false>
+// Sub (forward, direct only): the subtract-and-scale output of FusedArgs.
+template <class G, bool Fwd, bool Staged, class Arith, bool Mul = false, bool Sub = false>
 __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedArgs a) {
     static_assert(!Mul || (Fwd && !Staged), "the product epilogue follows a direct forward");
+    static_assert(!Sub || (Fwd && !Staged && !Mul), "the subtract-and-scale output follows a direct forward");
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t rank = (G::C > 1) ? cluster_rank() : 0u;
     const uint32_t cluster = blockIdx.x / G::C;
@@ -373,7 +435,7 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedA
         if (j0 < j1) issue_slab<G, Fwd>(a, j0, rank, stage_sa, mbar_sa);
     }
     static_assert(!Staged || G::NP == 1, "the staged schedule carries one polynomial per job");
-    DevCtx<G::C, Staged, G::NP, Mul> ctx;
+    DevCtx<G::C, Staged, G::NP, Mul, Sub> ctx;
     const uint32_t groups = (a.polys + G::NP - 1) / G::NP;
     ctx.smem = smem;
     ctx.stage = smem + G::STAGE_OFF_WORDS;
@@ -381,7 +443,8 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedA
     ctx.rank = rank;
     uint32_t parity = 0;
     for (uint32_t job = j0; job < j1; ++job, parity ^= 1u) {
-        const uint32_t limb = job / groups, poly0 = (job - limb * groups) * G::NP;
+        const uint32_t jl = job / groups, poly0 = (job - jl * groups) * G::NP;
+        const uint32_t limb = map_limb(a, jl);
         if constexpr (Mul) ctx.live = 0;
 #pragma unroll
         for (int p = 0; p < G::NP; ++p) {
@@ -401,6 +464,14 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedA
         ctx.twp = a.tw + ((size_t)limb << G::LOGN);
         ctx.q = __ldg(a.q + limb);
         ctx.q2 = 2u * ctx.q;
+        if constexpr (Sub) {
+#pragma unroll
+            for (int p = 0; p < G::NP; ++p) {
+                const SubJob sj = sub_job<G::LOGN>(a, limb, min(poly0 + p, a.polys - 1), ctx.q);
+                ctx.sb[p] = sj.base;
+                ctx.sub_e = sj.e;
+            }
+        }
         if (a.scale) ctx.scale_c = __ldg(a.scale + limb) % ctx.q;
         if constexpr (Mul) ctx.qinv = neg_qinv_dev(ctx.q);
         if constexpr (Staged) {

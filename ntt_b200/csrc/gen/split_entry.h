@@ -1,7 +1,8 @@
 // FusedConfig table entry of split configuration S(N, CL, EB, K2A, K2B)
 // (configs.h, split_kernel.cuh): one job per cluster, so both schedules run
 // the same direct launch; the forward with the product epilogue is left to a
-// cluster configuration (kern_mul null); kern_smul is the one-launch product.
+// cluster configuration (kern_mul null); kern_smul is the one-launch product,
+// kern_sub the forward with the subtract-and-scale output.
 #pragma once
 #include "../configs.h"
 #include "../split_kernel.cuh"
@@ -18,4 +19,6 @@
      {nullptr, nullptr}, 1, KB,                                                                  \
      {(const void*)&split_mul_kernel<NTTB_SG(N, CL, EB, KA, KB), Lazy4>,                         \
       (const void*)&split_mul_kernel<NTTB_SG(N, CL, EB, KA, KB), Lazy2>},                        \
-     SplitMulGeo<NTTB_SG(N, CL, EB, KA, KB)>::SMEM_BYTES},
+     SplitMulGeo<NTTB_SG(N, CL, EB, KA, KB)>::SMEM_BYTES,                                     \
+     {(const void*)&split_kernel<NTTB_SG(N, CL, EB, KA, KB), true, Lazy4, true>,                 \
+      (const void*)&split_kernel<NTTB_SG(N, CL, EB, KA, KB), true, Lazy2, true>}},

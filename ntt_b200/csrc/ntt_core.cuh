@@ -419,6 +419,13 @@ struct Maps {
 // Register-level stage loops.
 // ---------------------------------------------------------------------------
 
+// Whether a memory context reads compressed twiddle tables (tw_comp_*,
+// arith.cuh): Ctx::kCompTw when the context declares it, else false.
+template <class Ctx, class = void>
+struct CompTw : std::false_type {};
+template <class Ctx>
+struct CompTw<Ctx, std::void_t<decltype(Ctx::kCompTw)>> : std::bool_constant<Ctx::kCompTw> {};
+
 // Stage k of a pass.  CT (Fwd): acts on lambda bit p = PLO + KB - 1 - k,
 // groups = top k butterfly-coordinate bits.  GS: bit p = PLO + k, groups =
 // top KB-1-k butterfly bits.  `tbase` is the twiddle index of group 0 for
@@ -428,7 +435,10 @@ struct Maps {
 // same butterfly of all NP polynomials of the job.
 // Perm != 0: the stage's twiddle block (starting at index H) is stored
 // interleaved by Perm (tw_slot, arith.cuh): entry H + j at slot
-// H + (j % Perm) * S + j / Perm.
+// H + (j % Perm) * S + j / Perm.  With compressed tables (CompTw<Ctx>) the
+// table holds only the slots of j % Perm == 0 (the base block, at
+// (log2 Perm + 1) * S) and the 16 factors L (at 6 S): entry H + j is
+// base[j / Perm] * L[j % Perm].
 template <class L, class Arith, bool Fwd, int k, bool Fold, int NP, int Perm = 0,
           uint32_t H = 0, uint32_t S = 0, class Ctx>
 NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
@@ -457,8 +467,33 @@ NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
             constexpr int xh = decltype(XH)::value;
             constexpr uint32_t xoff = L::off(xh << XLB) >> (p + 1);
             // twiddles of this stage for this xh: 2^gbits consecutive entries
+            // (compressed: w holds the base factor and wl the unit-step one)
             TwPair w[1 << gbits];
-            if constexpr (Perm == 0) {
+            constexpr bool kComp = Perm != 0 && CompTw<Ctx>::value;
+            [[maybe_unused]] TwPair wl[kComp ? (1 << gbits) : 1] = {};
+            [[maybe_unused]] constexpr int lpc = Perm == 16 ? 4 : Perm == 8 ? 3 : Perm == 4 ? 2 : 1;
+            constexpr bool kAlignedC =
+                Perm != 0 &&
+                ((L::kRegMask >> (p + 1)) & (uint32_t)(Perm - 1)) == (uint32_t)(Perm - 1);
+            if constexpr (kComp) {
+                constexpr uint32_t CB = (uint32_t)(lpc + 1) * S, LB = 6u * S;
+                const uint32_t j0 = tbase - H;
+                if constexpr (kAlignedC) {
+                    auto tb = ctx.tw_base(CB + (j0 >> lpc));
+                    ct_for<(1 << gbits)>([&](auto Gc) {
+                        constexpr uint32_t c = xoff + decltype(Gc)::value;
+                        w[decltype(Gc)::value] = ctx.tw_ld(tb, c >> lpc);
+                        if constexpr ((c & (uint32_t)(Perm - 1)) != 0)
+                            wl[decltype(Gc)::value] = ctx.tw_at(LB + (c & (uint32_t)(Perm - 1)));
+                    });
+                } else {
+                    ct_for<(1 << gbits)>([&](auto Gc) {
+                        const uint32_t j = j0 + xoff + decltype(Gc)::value;
+                        w[decltype(Gc)::value] = ctx.tw_at(CB + (j >> lpc));
+                        wl[decltype(Gc)::value] = ctx.tw_at(LB + (j & (uint32_t)(Perm - 1)));
+                    });
+                }
+            } else if constexpr (Perm == 0) {
                 auto tb = ctx.tw_base(tbase + xoff);
                 if constexpr (gbits >= 1) {
                     ct_for<(1 << (gbits - 1))>([&](auto G2) {
@@ -494,6 +529,10 @@ NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
             }
             ct_for<(1 << gbits)>([&](auto Gc) {
                 constexpr int g = decltype(Gc)::value;
+                // group g needs the second factor (its unit-step index is
+                // known at compile time in the aligned case; L[0] = 1)
+                constexpr bool kTwo =
+                    kComp && (!kAlignedC || ((xoff + (uint32_t)g) & (uint32_t)(Perm - 1)) != 0);
                 ct_for<(1 << bbit)>([&](auto LO) {
                     constexpr int lo = decltype(LO)::value;
                     ct_for<(1 << XLB)>([&](auto XL) {
@@ -502,10 +541,16 @@ NTT_HD void stage(Ctx& ctx, uint32_t (&v)[NP][L::E], uint32_t tbase) {
                         constexpr int r = (bc << L::XB) | (xh << XLB) | xl;
                         ct_for<NP>([&](auto Pp) {
                             constexpr int pp = decltype(Pp)::value;
-                            if constexpr (Fwd)
+                            if constexpr (kTwo) {
+                                if constexpr (Fwd)
+                                    Arith::ct2(v[pp][r], v[pp][r + stride], w[g], wl[g], q, q2);
+                                else
+                                    Arith::gs2(v[pp][r], v[pp][r + stride], w[g], wl[g], q, q2);
+                            } else if constexpr (Fwd) {
                                 Arith::ct(v[pp][r], v[pp][r + stride], w[g].w, w[g].wp, q, q2);
-                            else
+                            } else {
                                 Arith::gs(v[pp][r], v[pp][r + stride], w[g].w, w[g].wp, q, q2);
+                            }
                         });
                     });
                 });

@@ -29,8 +29,9 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule);
 // One launch of a fused configuration under a schedule (NTT_SCHEDULE_*);
 // lazy2: some modulus is >= 2^30 (the [0, 2q) range discipline for all).
 // mul: the direct forward with the product epilogue (FusedArgs.src).
+// sub: the direct forward with the subtract-and-scale output (FusedArgs.sub).
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
-                          int schedule, bool lazy2, bool mul = false);
+                          int schedule, bool lazy2, bool mul = false, bool sub = false);
 ntt_status_t validate_modulus(int logN, ModulusConfig m, ModulusRuntime* rt);
 // Validates m and fills the twiddle-generation inputs of both directions
 // (entries 0/1 carry the folded Montgomery / N^{-1} R^{-1} factors).
@@ -42,9 +43,20 @@ ntt_status_t twiddle_gen_inputs(int logN, ModulusConfig m, TwGenLimb* fwd, TwGen
 // spectrum word already at its place in `a`.
 // scale (optional, device, one constant per limb): forward of c * x, or
 // c * inverse, folded into the limb's stage 0.
+// ops (optional): the limb map and the subtract-and-scale output of the
+// ModUp / ModDown forwards (FusedArgs); `limbs` then counts the launch's
+// limbs (the table's limbs minus skip_len).
+struct LimbOps {
+    uint32_t skip_at = 0, skip_len = 0;
+    const uint32_t* sub = nullptr;
+    size_t sub_stride = 0;
+    uint32_t sub_begin = 0, sub_end = 0;
+    const uint32_t* sub_mul = nullptr;
+};
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,
                            cudaStream_t s, uint32_t* status, int schedule, bool lazy2,
-                           const uint32_t* mul_src = nullptr, const uint32_t* scale = nullptr);
+                           const uint32_t* mul_src = nullptr, const uint32_t* scale = nullptr,
+                           const LimbOps* ops = nullptr);
 
 }  // namespace nttb

@@ -16,9 +16,10 @@ __device__ __forceinline__ TwPair small_scaled(TwPair t, uint32_t c, uint32_t q)
 
 // f0, f1: table entries 0 and 1 (the constants folded into stage 0), already
 // scaled by the launch's limb constant if it carries one.
+// sb (forward): the limb's subtrahend (nullptr: none), e its constant.
 template <class Arith, bool Fwd>
 __device__ void small_body(uint32_t* a, const TwPair* tw, uint32_t q, int logN, uint32_t* s,
-                           TwPair f0, TwPair f1) {
+                           TwPair f0, TwPair f1, const uint32_t* sb, TwPair e) {
     const uint32_t N = 1u << logN, half = N >> 1, q2 = 2u * q;
     for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) s[i] = a[i];
     __syncthreads();
@@ -47,15 +48,22 @@ __device__ void small_body(uint32_t* a, const TwPair* tw, uint32_t q, int logN, 
         }
         __syncthreads();
     }
-    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x)
-        a[i] = Fwd ? Arith::fwd_final(s[i], q, q2) : s[i];
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
+        if (Fwd) {
+            const uint32_t y = Arith::fwd_final(s[i], q, q2);
+            a[i] = sb ? sub_scaled(y, sb[i], e, q) : y;
+        } else {
+            a[i] = s[i];
+        }
+    }
 }
 
 template <bool Fwd>
 __global__ void small_kernel(SmallArgs p) {
     __shared__ uint32_t s[1u << kSmallMaxLogN];
     const uint32_t job = blockIdx.x;
-    const uint32_t limb = job % p.limbs, poly = job / p.limbs;
+    const uint32_t jl = job % p.limbs, poly = job / p.limbs;
+    const uint32_t limb = jl >= p.skip_at ? jl + p.skip_len : jl;
     uint32_t* a = p.data + (size_t)poly * p.poly_stride + ((size_t)limb << p.logN);
     const TwPair* tw = p.tw + ((size_t)limb << p.logN);
     const uint32_t q = p.q[limb];
@@ -65,8 +73,17 @@ __global__ void small_kernel(SmallArgs p) {
         f0 = small_scaled(f0, c, q);
         f1 = small_scaled(f1, c, q);
     }
-    if (q < (1u << 30)) small_body<Lazy4, Fwd>(a, tw, q, p.logN, s, f0, f1);
-    else small_body<Lazy2, Fwd>(a, tw, q, p.logN, s, f0, f1);
+    const uint32_t* sb = nullptr;
+    TwPair e{0u, 0u};
+    if (Fwd && p.sub && limb >= p.sub_begin && limb < p.sub_end) {
+        const uint32_t k = limb - p.sub_begin;
+        unsigned long long c = p.scale ? p.scale[limb] % q : 1ull;
+        if (p.sub_mul) c = c * (p.sub_mul[k] % q) % q;
+        e = TwPair{(uint32_t)c, (uint32_t)((c << 32) / q)};
+        sb = p.sub + (size_t)poly * p.sub_stride + ((size_t)k << p.logN);
+    }
+    if (q < (1u << 30)) small_body<Lazy4, Fwd>(a, tw, q, p.logN, s, f0, f1, sb, e);
+    else small_body<Lazy2, Fwd>(a, tw, q, p.logN, s, f0, f1, sb, e);
 }
 
 cudaError_t launch_small(const SmallArgs& a, bool fwd, cudaStream_t s) {

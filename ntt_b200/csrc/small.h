@@ -14,6 +14,12 @@ struct SmallArgs {
     unsigned long long poly_stride;
     int logN;
     const uint32_t* scale;  // optional per-limb constant folded into stage 0
+    // limb map and subtract-and-scale output: as FusedArgs (fused_kernel.cuh)
+    uint32_t skip_at, skip_len;
+    const uint32_t* sub;
+    unsigned long long sub_stride;
+    uint32_t sub_begin, sub_end;
+    const uint32_t* sub_mul;
 };
 cudaError_t launch_small(const SmallArgs& a, bool fwd, cudaStream_t s);
 }  // namespace nttb

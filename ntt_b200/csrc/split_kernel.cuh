@@ -104,9 +104,10 @@ __device__ __forceinline__ void split_sync() {
 // The cluster kernels' device context, with global loads that either stream
 // (phase-1 input, read once) or bypass L1 (words other CTAs of the cluster
 // rewrote after this SM may have cached their lines).
-template <int C>
-struct SplitCtx : DevCtx<C, false, 1, false> {
+template <int C, bool Sub = false>
+struct SplitCtx : DevCtx<C, false, 1, false, Sub> {
     bool cg = false;
+    const uint32_t* sb_final = nullptr;  // Sub: the subtrahend, armed for the last store
     __device__ __forceinline__ uint32_t g_ld(const uint32_t* b, uint32_t c) const {
         return cg ? __ldcg(b + c) : __ldca(b + c);
     }
@@ -174,6 +175,7 @@ __device__ __forceinline__ void split_forward_body(Ctx& ctx) {
         store_smem<P2C, X, G::SLAB_WORDS>(ctx, v, d);
     }
     split_sync<G::kChunkWarp>();  // the warp's chunk holds the words it wrote
+    if constexpr (Ctx::kSub) ctx.sb[0] = ctx.sb_final;  // phase 1 stored plain words
     slab_out<G, X>(ctx, tid);
 }
 
@@ -227,21 +229,25 @@ __device__ __forceinline__ void split_inverse_body(Ctx& ctx) {
 // per job): cluster c runs job c.  The launcher always gives one job per
 // cluster (the hardware schedules the clusters); a loop over several jobs
 // made the compiler keep per-thread addresses live across jobs and spill.
-template <class G, bool Fwd, class Arith>
+// Sub (forward only): the subtract-and-scale output of FusedArgs on the
+// final store.
+template <class G, bool Fwd, class Arith, bool Sub = false>
 __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) split_kernel(FusedArgs a) {
+    static_assert(!Sub || Fwd, "the subtract-and-scale output follows a forward");
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t rank = cluster_rank();
     const uint32_t cluster = blockIdx.x / G::C;
     const uint32_t j0 = cluster * a.jobs_per_cluster;
     const uint32_t j1 = min(j0 + a.jobs_per_cluster, a.jobs);
-    SplitCtx<G::C> ctx;
+    SplitCtx<G::C, Sub> ctx;
     ctx.smem = smem;
     ctx.stage = nullptr;
     ctx.smem_sa = (uint32_t)__cvta_generic_to_shared(smem);
     ctx.rank = rank;
     if (j1 > j0) {  // one job per cluster
         const uint32_t job = j0;
-        const uint32_t limb = job / a.polys, poly = job - limb * a.polys;
+        const uint32_t jl = job / a.polys, poly = job - jl * a.polys;
+        const uint32_t limb = map_limb(a, jl);
         ctx.o[0] = a.data + (size_t)poly * a.poly_stride + ((size_t)limb << G::LOGN);
         ctx.g[0] = ctx.o[0];
         ctx.twp = a.tw + ((size_t)limb << G::LOGN);
@@ -249,6 +255,12 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) split_kernel(FusedA
         ctx.q2 = 2u * ctx.q;
         ctx.scale_c = a.scale ? __ldg(a.scale + limb) % ctx.q : kNoScale;
         ctx.cg = false;
+        if constexpr (Sub) {
+            const SubJob sj = sub_job<G::LOGN>(a, limb, poly, ctx.q);
+            ctx.sb[0] = nullptr;
+            ctx.sb_final = sj.base;
+            ctx.sub_e = sj.e;
+        }
         if constexpr (Fwd) split_forward_body<G, Arith>(ctx);
         else split_inverse_body<G, Arith>(ctx);
     }

@@ -77,12 +77,19 @@ void emu_config(int i, int* out9) {
     out9[7] = entries()[i].threads;
     out9[8] = (int)entries()[i].smem;
 }
-// data: limbs * N words in place; tw_pairs: limbs * N (w, w') pairs.
-// mode bit 0: forward (else inverse); bit 1: direct input (else staged).
+// data: limbs * N words in place; tw_pairs: limbs * N (w, w') pairs, or
+// limbs * tw_comp_entries(logN) with mode bit 2.
+// mode bit 0: forward (else inverse); bit 1: direct input (else staged);
+// bit 2: direct input over compressed tables.
 int emu_transform(int i, int mode, uint32_t* data, const uint32_t* tw_pairs, const uint32_t* q,
                   int limbs, double* stats) {
     g_err.clear();
-    RunFn fn = (mode & 2) ? entries()[i].direct : entries()[i].staged;
+    RunFn fn = (mode & 4) ? entries()[i].comp : (mode & 2) ? entries()[i].direct
+                                                          : entries()[i].staged;
+    if (!fn) {
+        g_err = "no compressed-table form below logN 15";
+        return 1;
+    }
     return fn(mode & 1, data, tw_pairs, q, limbs, stats, g_err);
 }
 const char* emu_last_error() { return g_err.c_str(); }

@@ -56,9 +56,10 @@ struct EmuCluster {
 // word index (the pass code only adds offsets below 2^kPolyShift).
 constexpr uint32_t kPolyShift = 24;
 
-template <bool Staged>
+template <bool Staged, bool Comp = false>
 struct EmuCtx {
     static constexpr bool kStaged = Staged;
+    static constexpr bool kCompTw = Comp;  // compressed twiddle tables (arith.cuh)
     EmuCluster* cl;
     uint32_t** gp;  // the job's polynomials (limb words each)
     uint32_t glen;
@@ -256,9 +257,10 @@ extern uint32_t* g_dump;
 // Conflict degree of every warp-wide access of a step (emu.cu).
 void account(EmuCluster& cl, Stats& st);
 
-template <class G, class Arith, bool Fwd, bool Staged>
+template <class G, class Arith, bool Fwd, bool Staged, bool Comp = false>
 int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::string& err) {
-    using Ctx = EmuCtx<Staged>;
+    using Ctx = EmuCtx<Staged, Comp>;
+    constexpr uint32_t kTwLen = Comp ? tw_comp_entries(G::LOGN) : (1u << G::LOGN);
     EmuCluster cl;
     cl.C = G::C;
     cl.smem_words = G::SMEM_WORDS;
@@ -302,7 +304,7 @@ int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::strin
             }
     }
     auto mk = [&](uint32_t rank) {
-        Ctx c{&cl, gp.data(), 1u << G::LOGN, tw, 1u << G::LOGN, q, 2 * q, rank};
+        Ctx c{&cl, gp.data(), 1u << G::LOGN, tw, kTwLen, q, 2 * q, rank};
         c.gwrites = gw.data();
         return c;
     };
@@ -386,7 +388,7 @@ int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::strin
             std::vector<uint32_t> one(N);
             for (uint32_t i = 0; i < N; ++i) one[i] = limb[(N - 1 - i + p) % N];
             Stats st1;
-            if (run_limb<G1, Arith, Fwd, false>(one.data(), tw, q, st1, err)) return 1;
+            if (run_limb<G1, Arith, Fwd, false, Comp>(one.data(), tw, q, st1, err)) return 1;
             if (one != pw[p]) {
                 err = "polynomial " + std::to_string(p) + " of a job differs from its own transform";
                 return 1;
@@ -397,20 +399,23 @@ int run_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::strin
     return 0;
 }
 
-template <class G, bool Staged>
+// Comp: the direct passes over compressed tables (tw_comp_entries pairs per
+// limb instead of N).
+template <class G, bool Staged, bool Comp = false>
 int run_cfg(int fwd, uint32_t* data, const uint32_t* tw_pairs, const uint32_t* q, int limbs,
             double* stats, std::string& err) {
     Stats st;
     const size_t N = size_t{1} << G::LOGN;
+    const size_t TWS = Comp ? tw_comp_entries(G::LOGN) : N;
     for (int l = 0; l < limbs; ++l) {
-        const TwPair* tw = reinterpret_cast<const TwPair*>(tw_pairs) + l * N;
+        const TwPair* tw = reinterpret_cast<const TwPair*>(tw_pairs) + l * TWS;
         int rc;
         if (q[l] < (1u << 30))
-            rc = fwd ? run_limb<G, Lazy4, true, Staged>(data + l * N, tw, q[l], st, err)
-                     : run_limb<G, Lazy4, false, Staged>(data + l * N, tw, q[l], st, err);
+            rc = fwd ? run_limb<G, Lazy4, true, Staged, Comp>(data + l * N, tw, q[l], st, err)
+                     : run_limb<G, Lazy4, false, Staged, Comp>(data + l * N, tw, q[l], st, err);
         else
-            rc = fwd ? run_limb<G, Lazy2, true, Staged>(data + l * N, tw, q[l], st, err)
-                     : run_limb<G, Lazy2, false, Staged>(data + l * N, tw, q[l], st, err);
+            rc = fwd ? run_limb<G, Lazy2, true, Staged, Comp>(data + l * N, tw, q[l], st, err)
+                     : run_limb<G, Lazy2, false, Staged, Comp>(data + l * N, tw, q[l], st, err);
         if (rc) return rc;
     }
     if (stats) {
@@ -427,7 +432,15 @@ struct Entry {
     int threads;
     unsigned smem;
     RunFn staged, direct;
+    RunFn comp;  // direct, compressed tables (logN >= kTwCompMinLogN; else null)
 };
+
+// The compressed-table run of a geometry (none below kTwCompMinLogN).
+template <class G>
+constexpr RunFn comp_run() {
+    if constexpr (G::LOGN >= kTwCompMinLogN) return &run_cfg<G, false, true>;
+    else return nullptr;
+}
 
 // NP > 1 has no staged form: its staged entry runs the direct passes, as
 // the library's does.
@@ -437,5 +450,6 @@ struct Entry {
      EMU_G(N, CL, R1, EB, K1A, K2A, NP)::THREADS,                                          \
      EMU_G(N, CL, R1, EB, K1A, K2A, NP)::SMEM_BYTES,                                       \
      &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A, NP), (NP) == 1>,                              \
-     &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A, NP), false>},
+     &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A, NP), false>,                                  \
+     comp_run<EMU_G(N, CL, R1, EB, K1A, K2A, NP)>()},
 }  // namespace emu

@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from twiddle_ref import device_tables
+from twiddle_ref import COMP_MIN_LOGN, compressed_tables, device_tables
 
 EMU_DIR = os.path.join(os.path.dirname(__file__), "emu")
 
@@ -67,3 +67,47 @@ def test_config_matches_oracle(emu, idx, cfg, bits, direct):
     expect = x.copy()
     expect[0, 3] = 0xFFFFFFFF % T.q[0]
     assert np.array_equal(d, expect)
+
+
+@pytest.mark.parametrize("idx,cfg", [(i, c) for i, c in enumerate(configs())
+                                     if c[0] >= COMP_MIN_LOGN], ids=lambda v: str(v))
+@pytest.mark.parametrize("bits", [30, 31])
+def test_compressed_twiddles_match_oracle(emu, idx, cfg, bits):
+    """The compressed-table butterflies (two Shoup factors in the last four
+    stages, aligned and unaligned index paths) over every configuration of
+    logN >= 15: bit-exact against the oracle, in bounds, exactly-once."""
+    logN = cfg[0]
+    start = int(2 ** 29.5) if bits == 30 else int(2 ** 30.5)
+    mods = O.ascending_primes(logN, 2, start)
+    T = O.LimbTables(logN, mods)
+    fwd, inv = compressed_tables(T)
+    assert fwd.shape[1] == 3 * (1 << logN) // 16 + 16
+    x = O.uniform_limbs(logN, T.q, 300 + idx)
+    x[1, :3] = [0, T.q[1] - 1, 0xFFFFFFFF]
+    d = x.copy()
+    st = (ctypes.c_double * 2)()
+    rc = emu.emu_transform(idx, 1 | 4, d.ctypes.data, fwd.ctypes.data, T.q.ctypes.data, 2, st)
+    assert rc == 0, emu.emu_last_error().decode()
+    assert np.array_equal(d, T.forward_mont(x))
+    rc = emu.emu_transform(idx, 0 | 4, d.ctypes.data, inv.ctypes.data, T.q.ctypes.data, 2, st)
+    assert rc == 0, emu.emu_last_error().decode()
+    expect = x.copy()
+    expect[1, 2] = 0xFFFFFFFF % T.q[1]
+    assert np.array_equal(d, expect)
+
+
+def test_compressed_tables_factor_the_full_ones():
+    """Every entry of the last four stages is its base entry times its
+    unit-step factor (mod q): the identity the compressed layout rests on."""
+    for logN in (15, 16, 17):
+        mods = O.ascending_primes(logN, 1, int(2 ** 30.5))
+        T = O.LimbTables(logN, mods)
+        q = T.q[0]
+        N = 1 << logN
+        for tab in (T.psi_tab[0], T.inv_tab[0]):
+            for p in range(4):
+                h, f = N >> (p + 1), 16 >> p
+                j = np.arange(N >> (p + 1), dtype=np.uint64)
+                base = tab[h + (j // f) * f].astype(np.uint64)
+                lsb = tab[(j % f)].astype(np.uint64)
+                assert np.array_equal((base * lsb) % np.uint64(q), tab[h + j].astype(np.uint64))

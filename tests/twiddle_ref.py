@@ -58,3 +58,33 @@ def device_tables(T):
     pf[:, slots] = fwd
     pi[:, slots] = inv
     return pf, pi
+
+
+COMP_MIN_LOGN = 15
+
+
+def compressed_tables(T):
+    """The compressed layout (arith.cuh, tw_comp_*) of T's device tables:
+    uint32[L, 3N/16 + 16, 2] per direction -- entries 0 .. N/16-1 as in the
+    full table (folded 0 and 1 included), then for p = 3, 2, 1, 0 the base
+    block of stage logN-1-p (entry H + m F, H = N / 2^(p+1), F = 16 / 2^p,
+    m < N/32), then the unit-step factors psi^(+-bitrev(c)), c < 16, with
+    factor 0 = 1 (never folded)."""
+    fwd_s, inv_s = device_tables(T)
+    L, N = T.psi_tab.shape
+    logN = T.logN
+    slots = np.array([tw_slot(i, logN) for i in range(N)])
+    fwd, inv = fwd_s[:, slots], inv_s[:, slots]  # natural order, folds kept
+    idx = list(range(N // 16))
+    for p in (3, 2, 1, 0):
+        h, f = N >> (p + 1), 16 >> p
+        idx += [h + m * f for m in range(N // 32)]
+    out = []
+    for full, tab in ((fwd, T.psi_tab), (inv, T.inv_tab)):
+        c = np.empty((L, len(idx) + 16, 2), dtype=np.uint32)
+        c[:, :len(idx)] = full[:, idx]
+        for l, (q, _) in enumerate(T.moduli):
+            for k in range(16):
+                c[l, len(idx) + k] = _pair(int(tab[l, k]), q)
+        out.append(c)
+    return out[0], out[1]
