@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=5)
     ap.add_argument("--no-multiply", action="store_true")
     ap.add_argument("--multiply-steps", type=int, default=10)
+    ap.add_argument("--no-compressed", action="store_true")
+    ap.add_argument("--compressed-steps", type=int, default=50)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=20000)
     ap.add_argument("--serve-loads", type=str, default="0.5,0.8,0.95")
@@ -423,6 +425,8 @@ def run_ours(args):
                                            out["batched"]["polynomials"])
     if not args.no_multiply:
         out["fused_multiply"] = bench_multiply(args, torch, nb, stream)
+    if not args.no_compressed:
+        out["compressed_twiddles"] = bench_compressed(args, torch, nb, stream, d, P)
     if not args.no_serve:
         out["serve"] = bench_serve(args, torch, nb)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -456,6 +460,10 @@ def summary(out):
         fm = out["fused_multiply"]
         s["multiply_speedup_vs_unfused"] = r(fm["speedup_vs_unfused"])
         s["multiply_batch_tiles_speedup_vs_unfused"] = r(fm["batch_tiles"]["speedup_vs_unfused"])
+    if "compressed_twiddles" in out:
+        ct = out["compressed_twiddles"]
+        s["compressed_headline_ratio"] = r(ct["headline"]["speedup_vs_full"])
+        s["compressed_table_bound_ratio"] = r(ct["table_bound"]["speedup_vs_full"])
     if "serve" in out:
         for leg in ("host", "device"):
             L = out["serve"][leg]
@@ -470,6 +478,91 @@ def summary(out):
 
 
 RAGGED = dict(seed=SEED, count=256, logn=tuple(range(12, 17)), limbs=(1, 48), bits=(30,))
+
+
+def bench_compressed(args, torch, nb, stream, d, P):
+    """Full against compressed twiddle tables (NTT_PLAN_COMPRESSED_TWIDDLES:
+    3N/16 + 16 pairs per limb instead of N, the last four stages multiplying
+    by two factors).  Two workloads, device-resident, step = forward +
+    inverse, CUDA events:
+      headline: the headline batch (64 x 2^16 x 16 limbs; 16 MiB of full
+        tables, L2-resident either way): the compute cost of compression;
+      table_bound: 4 plans of disjoint 32-limb chains of 30-bit primes at
+        logN 17, one polynomial per call through each plan in turn (the
+        per-ciphertext pattern of RNS schemes): full tables 4 x 2 x 32 MiB =
+        256 MiB cycle through the 126 MB L2, compressed ones 48 MiB.
+    Both forms give the same words (checked)."""
+    sh = stream.cuda_stream
+    K = args.compressed_steps
+    res = {}
+    # headline workload
+    mods = moduli()
+    pf = nb.Plan(16, mods)
+    pc = nb.Plan(16, mods, compressed_twiddles=True)
+    x = d.clone()
+    with torch.cuda.stream(stream):
+        pc.forward_many(x, P, 0, sh)
+    y = d.clone()
+    with torch.cuda.stream(stream):
+        pf.forward_many(y, P, 0, sh)
+    stream.synchronize()
+    if not torch.equal(x, y):
+        raise RuntimeError("compressed and full tables differ (headline)")
+    del y
+
+    def step(p):
+        return lambda: (p.forward_many(x, P, 0, sh), p.inverse_many(x, P, 0, sh))
+    t_full = device_time(torch, stream, step(pf), K, 3)
+    t_comp = device_time(torch, stream, step(pc), K, 3)
+    res["headline"] = {"workload": f"{P} x 2^16 x 16 limbs (default moduli), forward + inverse",
+                       "full_ms": t_full, "compressed_ms": t_comp,
+                       "speedup_vs_full": t_full / t_comp,
+                       "table_bytes_full": pf.info.device_bytes,
+                       "table_bytes_compressed": pc.info.device_bytes}
+    pf.close()
+    pc.close()
+    # table-bound workload
+    logN, limbs, chains = 17, 32, 4
+    # disjoint chains: 32 primes q = 1 mod 2^18 span < 2^27, all below 2^30
+    starts = [(1 << 29) + k * (1 << 27) for k in range(chains)]
+    chain = [nb.find_moduli(logN, limbs, s0) for s0 in starts]
+    plans_f = [nb.Plan(logN, c) for c in chain]
+    plans_c = [nb.Plan(logN, c, compressed_twiddles=True) for c in chain]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    polys = [torch.randint(0, 1 << 29, (limbs << logN,), generator=g, device="cuda",
+                           dtype=torch.int32) for _ in range(chains)]
+    chk = [p.clone() for p in polys]
+    with torch.cuda.stream(stream):
+        for p, v in zip(plans_c, polys):
+            p.forward(v, sh)
+        for p, v in zip(plans_f, chk):
+            p.forward(v, sh)
+    stream.synchronize()
+    if not all(torch.equal(a, b) for a, b in zip(polys, chk)):
+        raise RuntimeError("compressed and full tables differ (table-bound)")
+    del chk
+
+    def cycle(plans):
+        def fn():
+            for p, v in zip(plans, polys):
+                p.forward(v, sh)
+                p.inverse(v, sh)
+        return fn
+    t_full = device_time(torch, stream, cycle(plans_f), K, 3)
+    t_comp = device_time(torch, stream, cycle(plans_c), K, 3)
+    res["table_bound"] = {
+        "workload": f"{chains} chains x 2^{logN} x {limbs} limbs of 30-bit primes, one "
+                    "polynomial per call, forward + inverse through each plan in turn",
+        "full_ms": t_full, "compressed_ms": t_comp, "speedup_vs_full": t_full / t_comp,
+        "limb_ntt_per_s_full": 2 * chains * limbs / (t_full / 1000.0),
+        "limb_ntt_per_s_compressed": 2 * chains * limbs / (t_comp / 1000.0),
+        "table_bytes_full": sum(p.info.device_bytes for p in plans_f),
+        "table_bytes_compressed": sum(p.info.device_bytes for p in plans_c)}
+    for p in plans_f + plans_c:
+        p.close()
+    res["steps"] = K
+    return res
 
 
 def device_time(torch, stream, fn, steps, warmup):

@@ -130,6 +130,8 @@ typedef struct ntt_plan_info {
     int tuned;              /* 1 if the configuration came from the tuner   */
     int fwd_config;         /* catalogue index (ntt_config_get) of the      */
     int inv_config;         /* forward / inverse kernel; -1: small sizes    */
+    int twiddle_entries;    /* (w, w') pairs per limb and direction: N, or
+                               3N/16 + 16 with compressed tables            */
 } ntt_plan_info_t;
 
 /* Validates every (qi, primitive_root) exactly as make_modulus_runtime does
@@ -140,6 +142,25 @@ typedef struct ntt_plan_info {
  * kernel configurations (results do not depend on it). */
 NTT_API ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int limbs,
                              const TransformConfig* transform, ntt_plan_t** out);
+
+/* Plan options (flags of ntt_plan_create_ex). */
+/* Compressed twiddle tables (Cheddar's on-the-fly twiddles, an MSB x LSB
+ * table product: src/NTT_cheddar.cu:42-43, 80-84, 1283-1289): per limb and
+ * direction 3N/16 + 16 pairs instead of N (5.3x fewer table bytes): the
+ * entries of the first logN-4 stages, one base entry per run of 16 / 8 / 4 /
+ * 2 consecutive entries of each of the last four stages, and 16 unit-step
+ * factors; those stages multiply by the two factors in turn (two Shoup
+ * products instead of one).  The trade: ~20% more integer multiplies per
+ * transform for tables that stay in L2 when many limbs or moduli are in
+ * flight.  logN >= 15 (the split kernels); such plans run ntt_forward /
+ * ntt_inverse (_many, _scaled, _skip, _scaled_range) and return
+ * NTT_ERR_UNSUPPORTED for ntt_forward_sub_scale and ntt_multiply_many.
+ * Results are identical to those of a full-table plan. */
+#define NTT_PLAN_COMPRESSED_TWIDDLES 1u
+/* ntt_plan_create with option flags (0 = ntt_plan_create). */
+NTT_API ntt_status_t ntt_plan_create_ex(int logN, const ModulusConfig* moduli, int limbs,
+                                        const TransformConfig* transform, uint32_t flags,
+                                        ntt_plan_t** out);
 NTT_API ntt_status_t ntt_plan_destroy(ntt_plan_t* plan);
 NTT_API ntt_status_t ntt_plan_get_info(const ntt_plan_t* plan, ntt_plan_info_t* out);
 /* Waits for the device, then reads and clears the plan's device status word

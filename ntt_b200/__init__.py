@@ -80,7 +80,8 @@ class PlanInfo(ctypes.Structure):
     _fields_ = [("logN", ctypes.c_int), ("limbs", ctypes.c_int), ("cluster_ctas", ctypes.c_int),
                 ("threads_per_cta", ctypes.c_int), ("smem_bytes", ctypes.c_uint32),
                 ("effective", TransformConfig), ("device_bytes", ctypes.c_size_t),
-                ("tuned", ctypes.c_int), ("fwd_config", ctypes.c_int), ("inv_config", ctypes.c_int)]
+                ("tuned", ctypes.c_int), ("fwd_config", ctypes.c_int), ("inv_config", ctypes.c_int),
+                ("twiddle_entries", ctypes.c_int)]
 
 
 class KernelConfig(ctypes.Structure):
@@ -98,6 +99,7 @@ class TuneResult(ctypes.Structure):
 
 
 NTT_OK = 0
+PLAN_COMPRESSED_TWIDDLES = 1  # include/ntt_b200.h: NTT_PLAN_COMPRESSED_TWIDDLES
 STATUS_NAMES = {
     0: "NTT_OK", 1: "NTT_ERR_INVALID_ARGUMENT", 2: "NTT_ERR_MODULUS", 3: "NTT_ERR_ROOT",
     4: "NTT_ERR_MODULUS_RANGE", 5: "NTT_ERR_UNSUPPORTED", 6: "NTT_ERR_MISALIGNED",
@@ -140,6 +142,8 @@ _sig("ntt_find_moduli", _st, ctypes.c_int, ctypes.c_int, ctypes.c_uint32,
      ctypes.POINTER(ModulusConfig))
 _sig("ntt_plan_create", _st, ctypes.c_int, ctypes.POINTER(ModulusConfig), ctypes.c_int,
      ctypes.POINTER(TransformConfig), ctypes.POINTER(_vp))
+_sig("ntt_plan_create_ex", _st, ctypes.c_int, ctypes.POINTER(ModulusConfig), ctypes.c_int,
+     ctypes.POINTER(TransformConfig), ctypes.c_uint32, ctypes.POINTER(_vp))
 _sig("ntt_plan_destroy", _st, _vp)
 _sig("ntt_plan_get_info", _st, _vp, ctypes.POINTER(PlanInfo))
 _sig("ntt_plan_tables", _st, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp))
@@ -273,12 +277,14 @@ class Plan:
     modulus chain).  Immutable after creation; usable from several host
     threads on different streams."""
 
-    def __init__(self, logN: int, moduli: Sequence, transform: Optional[TransformConfig] = None):
+    def __init__(self, logN: int, moduli: Sequence, transform: Optional[TransformConfig] = None,
+                 compressed_twiddles: bool = False):
         arr, n = _moduli_array(moduli)
         h = _vp()
-        _check(_lib.ntt_plan_create(logN, arr, n,
-                                    ctypes.byref(transform) if transform is not None else None,
-                                    ctypes.byref(h)), "ntt_plan_create")
+        flags = PLAN_COMPRESSED_TWIDDLES if compressed_twiddles else 0
+        _check(_lib.ntt_plan_create_ex(logN, arr, n,
+                                       ctypes.byref(transform) if transform is not None else None,
+                                       flags, ctypes.byref(h)), "ntt_plan_create_ex")
         self._h = h
         self.logN = logN
         self.N = 1 << logN

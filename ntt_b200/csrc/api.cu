@@ -178,9 +178,10 @@ static uint32_t smem_of(const FusedConfig* c, int schedule) {
 }
 
 static const void* kernel_of(const FusedConfig* c, bool fwd, int schedule, bool lazy2,
-                             bool mul = false, bool sub = false) {
+                             bool mul = false, bool sub = false, bool comp = false) {
     if (mul) return c->kern_mul[lazy2 ? 1 : 0];
     if (sub) return c->kern_sub[lazy2 ? 1 : 0];
+    if (comp) return c->kern_comp[fwd ? 1 : 0][lazy2 ? 1 : 0];
     return c->kernel(schedule == NTT_SCHEDULE_STAGED, fwd, lazy2);
 }
 
@@ -252,11 +253,12 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule) {
 // wave of resident clusters, each running a contiguous chunk of limb-major
 // jobs with the next input slab bulk-copied ahead.
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
-                          int schedule, bool lazy2, bool mul, bool sub) {
+                          int schedule, bool lazy2, bool mul, bool sub, bool comp) {
     if (a.jobs == 0) return NTT_OK;
     // the output epilogues and the split kernels have a direct form only
     if (mul || sub || c->split) schedule = NTT_SCHEDULE_DIRECT;
-    const void* fn = kernel_of(c, fwd, schedule, lazy2, mul, sub);
+    const void* fn = kernel_of(c, fwd, schedule, lazy2, mul, sub, comp);
+    if (!fn) return fail(NTT_ERR_UNSUPPORTED, "configuration has no such kernel");
     ntt_status_t st = prepare_function(c, fn, schedule);
     if (st != NTT_OK) return st;
     const unsigned C = 1u << c->clog;
@@ -313,6 +315,8 @@ struct ntt_plan {
     int tuned = 0;
     int schedule = NTT_SCHEDULE_DIRECT;
     bool lazy2 = false;  // a modulus >= 2^30: every limb uses the [0, 2q) discipline
+    bool compressed = false;  // compressed twiddle tables (split configurations only)
+    size_t tw_stride = 0;     // table pairs per limb: N, or tw_comp_entries(logN)
 };
 
 namespace nttb {
@@ -389,6 +393,16 @@ void choose_configs(ntt_plan* p, const TransformConfig* t) {
     // single-polynomial launches: an explicit phase split still applies
     p->cfg_fwd1 = (t && p->cfg_fwd->np == 1) ? p->cfg_fwd : default_single_config(p->logN, true);
     p->cfg_inv1 = (t && p->cfg_inv->np == 1) ? p->cfg_inv : default_single_config(p->logN, false);
+    // compressed tables: only configurations with those kernels (split)
+    if (p->compressed) {
+        auto keep = [&](const FusedConfig*& c, bool fwd) {
+            if (!c || !c->kern_comp[0][0]) c = default_config(p->logN, fwd);
+        };
+        keep(p->cfg_fwd, true);
+        keep(p->cfg_inv, false);
+        keep(p->cfg_fwd1, true);
+        keep(p->cfg_inv1, false);
+    }
 }
 
 }  // namespace nttb
@@ -475,12 +489,27 @@ ntt_status_t ntt_find_moduli(int logN, int count, uint32_t lower_bound, ModulusC
 
 ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int limbs,
                              const TransformConfig* transform, ntt_plan_t** out) {
+    return ntt_plan_create_ex(logN, moduli, limbs, transform, 0u, out);
+}
+
+ntt_status_t ntt_plan_create_ex(int logN, const ModulusConfig* moduli, int limbs,
+                                const TransformConfig* transform, uint32_t flags,
+                                ntt_plan_t** out) {
     if (!out) return fail(NTT_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
     if (logN < NTT_MIN_LOGN || logN > NTT_MAX_LOGN)
         return fail(NTT_ERR_UNSUPPORTED, "logN %d outside [%d, %d]", logN, NTT_MIN_LOGN,
                     NTT_MAX_LOGN);
     if (limbs < 1 || !moduli) return fail(NTT_ERR_INVALID_ARGUMENT, "need at least one modulus limb");
+    if (flags & ~NTT_PLAN_COMPRESSED_TWIDDLES)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "unknown plan flags 0x%x", flags);
+    const bool compressed = (flags & NTT_PLAN_COMPRESSED_TWIDDLES) != 0;
+    if (compressed) {
+        const FusedConfig* d = logN >= kTwCompMinLogN ? default_config(logN, true) : nullptr;
+        if (!d || !d->kern_comp[0][0])
+            return fail(NTT_ERR_UNSUPPORTED, "compressed twiddle tables need logN >= %d (logN %d)",
+                        kTwCompMinLogN, logN);
+    }
     if (ntt_status_t st = check_transform(logN, transform)) return st;
     std::vector<TwGenLimb> gf(limbs), gi(limbs);
     std::vector<uint32_t> qh(limbs);
@@ -494,8 +523,10 @@ ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int limbs,
     p->limbs = limbs;
     p->moduli.assign(moduli, moduli + limbs);
     for (int l = 0; l < limbs; ++l) p->lazy2 |= moduli[l].qi >= (1u << 30);
+    p->compressed = compressed;
+    p->tw_stride = compressed ? tw_comp_entries(logN) : N;
     cudaError_t e = cudaGetDevice(&p->device);
-    const size_t tw_bytes = (size_t)limbs * N * sizeof(TwPair);
+    const size_t tw_bytes = ((size_t)limbs * p->tw_stride * sizeof(TwPair) + 255) & ~(size_t)255;
     const size_t q_bytes = ((size_t)limbs * 4 + 255) & ~(size_t)255;
     p->bytes = 2 * tw_bytes + q_bytes + 256;
     if (e == cudaSuccess) e = cudaMalloc(&p->block, p->bytes);
@@ -512,8 +543,9 @@ ntt_status_t ntt_plan_create(int logN, const ModulusConfig* moduli, int limbs,
     if (e == cudaSuccess) e = cudaMemcpy(gdev, gf.data(), limbs * sizeof(TwGenLimb), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(gdev + limbs, gi.data(), limbs * sizeof(TwGenLimb), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = launch_twiddle_gen(p->fwd, gdev, limbs, logN, 0);
-    if (e == cudaSuccess) e = launch_twiddle_gen(p->inv, gdev + limbs, limbs, logN, 0);
+    auto gen = compressed ? launch_twiddle_gen_comp : launch_twiddle_gen;
+    if (e == cudaSuccess) e = gen(p->fwd, gdev, limbs, logN, 0);
+    if (e == cudaSuccess) e = gen(p->inv, gdev + limbs, limbs, logN, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (gdev) cudaFree(gdev);
     if (e != cudaSuccess) {
@@ -561,6 +593,7 @@ ntt_status_t ntt_plan_get_info(const ntt_plan_t* p, ntt_plan_info_t* out) {
     out->tuned = p->tuned;
     out->fwd_config = p->cfg_fwd ? (int)(p->cfg_fwd - fused_configs()) : -1;
     out->inv_config = p->cfg_inv ? (int)(p->cfg_inv - fused_configs()) : -1;
+    out->twiddle_entries = (int)p->tw_stride;
     return NTT_OK;
 }
 
@@ -571,6 +604,9 @@ ntt_status_t ntt_plan_force_config(ntt_plan_t* p, int fwd_index, int inv_index) 
     if ((fwd_index >= 0 && (!f || f->logN != p->logN)) ||
         (inv_index >= 0 && (!i || i->logN != p->logN)))
         return fail(NTT_ERR_INVALID_ARGUMENT, "configuration index does not match logN %d", p->logN);
+    if (p->compressed && (!f->kern_comp[0][0] || !i->kern_comp[0][0]))
+        return fail(NTT_ERR_INVALID_ARGUMENT,
+                    "compressed twiddle tables run on split configurations only");
     p->cfg_fwd = f;
     p->cfg_inv = i;
     p->cfg_fwd1 = f;  // a pinned configuration runs every launch
@@ -649,6 +685,11 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
     static const LimbOps kNone{};
     if (!ops) ops = &kNone;
     const bool sub = ops->sub != nullptr;
+    if (ops->compressed && (mul_src || sub))
+        return fail(NTT_ERR_UNSUPPORTED,
+                    "plans with compressed twiddle tables run plain and scaled transforms only");
+    if (ops->compressed && (!cfg || !cfg->kern_comp[0][0]))
+        return fail(NTT_ERR_UNSUPPORTED, "no compressed-table kernel for this configuration");
     if (polys == 0 || limbs == 0) return NTT_OK;
     if (!a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL data pointer");
     if (sub && (!fwd || mul_src))
@@ -685,7 +726,8 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
                      scale, ops->skip_at, ops->skip_len, ops->sub,
                      (unsigned long long)ops->sub_stride, ops->sub_begin, ops->sub_end,
                      ops->sub_mul};
-        return launch_fused(cfg, fwd, fa, s, schedule, lazy2, mul_src != nullptr, sub);
+        return launch_fused(cfg, fwd, fa, s, schedule, lazy2, mul_src != nullptr, sub,
+                            ops->compressed);
     }
     SmallArgs sa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride, logN,
                  scale, ops->skip_at, ops->skip_len, ops->sub,
@@ -711,10 +753,13 @@ static ntt_status_t plan_run(const ntt_plan_t* p, uint32_t* a, size_t polys, siz
     if (limb_end < 0) limb_end = p->limbs;
     const size_t off = (size_t)limb_begin << p->logN;
     int launch_limbs = limb_end - limb_begin;
-    if (ops) launch_limbs -= (int)ops->skip_len;
-    return run_transform(p->logN, cfg, (fwd ? p->fwd : p->inv) + off, p->q + limb_begin,
-                         launch_limbs, a ? a + off : nullptr, polys, stride, fwd,
-                         (cudaStream_t)s, p->status, p->schedule, p->lazy2, nullptr, scale, ops);
+    LimbOps o = ops ? *ops : LimbOps{};
+    o.compressed = p->compressed;
+    launch_limbs -= (int)o.skip_len;
+    return run_transform(p->logN, cfg, (fwd ? p->fwd : p->inv) + (size_t)limb_begin * p->tw_stride,
+                         p->q + limb_begin, launch_limbs, a ? a + off : nullptr, polys, stride,
+                         fwd, (cudaStream_t)s, p->status, p->schedule, p->lazy2, nullptr, scale,
+                         &o);
 }
 
 // The extent in words of `polys` polynomials of `limbs` limbs `stride` apart.
@@ -870,6 +915,8 @@ ntt_status_t ntt_multiply_many(const ntt_plan_t* p, const uint32_t* a, uint32_t*
     if (!p || !a || !b) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL argument");
     if (!p->cfg_fwd || !p->cfg_inv)
         return fail(NTT_ERR_UNSUPPORTED, "the fused product needs logN >= 10 (plan has %d)", p->logN);
+    if (p->compressed)
+        return fail(NTT_ERR_UNSUPPORTED, "plans with compressed twiddle tables have no fused product");
     if (stride == 0) stride = (size_t)p->limbs << p->logN;
     if (polys == 0) return NTT_OK;
     // checked before the first launch, so a refused call leaves b untouched

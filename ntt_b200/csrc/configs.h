@@ -68,6 +68,10 @@ struct FusedConfig {
     // the direct forward with the subtract-and-scale output (ModDown;
     // FusedArgs.sub): [lazy2]
     const void* kern_sub[2];
+    // split: the transforms over compressed twiddle tables (plans created
+    // with NTT_PLAN_COMPRESSED_TWIDDLES) [fwd][lazy2]; null for cluster
+    // configurations
+    const void* kern_comp[2][2];
     bool has_mul() const { return kern_mul[0] != nullptr; }
     const void* kernel(bool staged, bool fwd, bool lazy2) const {
         return kern[staged ? 1 : 0][fwd ? 1 : 0][lazy2 ? 1 : 0];

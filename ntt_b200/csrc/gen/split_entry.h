@@ -2,13 +2,16 @@
 // (configs.h, split_kernel.cuh): one job per cluster, so both schedules run
 // the same direct launch; the forward with the product epilogue is left to a
 // cluster configuration (kern_mul null); kern_smul is the one-launch product,
-// kern_sub the forward with the subtract-and-scale output.
+// kern_sub the forward with the subtract-and-scale output, kern_comp the
+// transforms over compressed twiddle tables.
 #pragma once
 #include "../configs.h"
 #include "../split_kernel.cuh"
 
 #define NTTB_SG(N, CL, EB, KA, KB) SplitGeo<N, CL, EB, KA, KB>
 #define NTTB_SK(N, CL, EB, KA, KB, F, A) (const void*)&split_kernel<NTTB_SG(N, CL, EB, KA, KB), F, A>
+#define NTTB_SKC(N, CL, EB, KA, KB, F, A) \
+    (const void*)&split_kernel<NTTB_SG(N, CL, EB, KA, KB), F, A, false, true>
 #define NTTB_SPLIT_ENTRY(N, CL, EB, KA, KB)                                                     \
     {N, CL, EB, EB, EB, KA, 1, NTTB_SG(N, CL, EB, KA, KB)::THREADS,                              \
      NTTB_SG(N, CL, EB, KA, KB)::SMEM_BYTES, NTTB_SG(N, CL, EB, KA, KB)::SMEM_BYTES,            \
@@ -21,4 +24,6 @@
       (const void*)&split_mul_kernel<NTTB_SG(N, CL, EB, KA, KB), Lazy2>},                        \
      SplitMulGeo<NTTB_SG(N, CL, EB, KA, KB)>::SMEM_BYTES,                                     \
      {(const void*)&split_kernel<NTTB_SG(N, CL, EB, KA, KB), true, Lazy4, true>,                 \
-      (const void*)&split_kernel<NTTB_SG(N, CL, EB, KA, KB), true, Lazy2, true>}},
+      (const void*)&split_kernel<NTTB_SG(N, CL, EB, KA, KB), true, Lazy2, true>},                \
+     {{NTTB_SKC(N, CL, EB, KA, KB, false, Lazy4), NTTB_SKC(N, CL, EB, KA, KB, false, Lazy2)},     \
+      {NTTB_SKC(N, CL, EB, KA, KB, true, Lazy4), NTTB_SKC(N, CL, EB, KA, KB, true, Lazy2)}}},

@@ -30,8 +30,10 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule);
 // lazy2: some modulus is >= 2^30 (the [0, 2q) range discipline for all).
 // mul: the direct forward with the product epilogue (FusedArgs.src).
 // sub: the direct forward with the subtract-and-scale output (FusedArgs.sub).
+// comp: the kernels over compressed twiddle tables (split configurations).
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
-                          int schedule, bool lazy2, bool mul = false, bool sub = false);
+                          int schedule, bool lazy2, bool mul = false, bool sub = false,
+                          bool comp = false);
 ntt_status_t validate_modulus(int logN, ModulusConfig m, ModulusRuntime* rt);
 // Validates m and fills the twiddle-generation inputs of both directions
 // (entries 0/1 carry the folded Montgomery / N^{-1} R^{-1} factors).
@@ -44,14 +46,16 @@ ntt_status_t twiddle_gen_inputs(int logN, ModulusConfig m, TwGenLimb* fwd, TwGen
 // scale (optional, device, one constant per limb): forward of c * x, or
 // c * inverse, folded into the limb's stage 0.
 // ops (optional): the limb map and the subtract-and-scale output of the
-// ModUp / ModDown forwards (FusedArgs); `limbs` then counts the launch's
-// limbs (the table's limbs minus skip_len).
+// ModUp / ModDown forwards (FusedArgs), and whether `tw` is a compressed
+// table (tw_comp_* layout); `limbs` counts the launch's limbs (the table's
+// limbs minus skip_len).
 struct LimbOps {
     uint32_t skip_at = 0, skip_len = 0;
     const uint32_t* sub = nullptr;
     size_t sub_stride = 0;
     uint32_t sub_begin = 0, sub_end = 0;
     const uint32_t* sub_mul = nullptr;
+    bool compressed = false;
 };
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,

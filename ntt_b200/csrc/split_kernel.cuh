@@ -104,8 +104,9 @@ __device__ __forceinline__ void split_sync() {
 // The cluster kernels' device context, with global loads that either stream
 // (phase-1 input, read once) or bypass L1 (words other CTAs of the cluster
 // rewrote after this SM may have cached their lines).
-template <int C, bool Sub = false>
+template <int C, bool Sub = false, bool Comp = false>
 struct SplitCtx : DevCtx<C, false, 1, false, Sub> {
+    static constexpr bool kCompTw = Comp;  // compressed twiddle tables (arith.cuh)
     bool cg = false;
     const uint32_t* sb_final = nullptr;  // Sub: the subtrahend, armed for the last store
     __device__ __forceinline__ uint32_t g_ld(const uint32_t* b, uint32_t c) const {
@@ -230,16 +231,19 @@ __device__ __forceinline__ void split_inverse_body(Ctx& ctx) {
 // cluster (the hardware schedules the clusters); a loop over several jobs
 // made the compiler keep per-thread addresses live across jobs and spill.
 // Sub (forward only): the subtract-and-scale output of FusedArgs on the
-// final store.
-template <class G, bool Fwd, class Arith, bool Sub = false>
+// final store.  Comp: compressed twiddle tables (tw_comp_entries pairs per
+// limb; the last four stages multiply by two factors).
+template <class G, bool Fwd, class Arith, bool Sub = false, bool Comp = false>
 __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) split_kernel(FusedArgs a) {
     static_assert(!Sub || Fwd, "the subtract-and-scale output follows a forward");
+    static_assert(!Comp || G::LOGN >= kTwCompMinLogN, "compressed tables start at logN 15");
+    constexpr uint32_t kTwStride = Comp ? tw_comp_entries(G::LOGN) : (1u << G::LOGN);
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t rank = cluster_rank();
     const uint32_t cluster = blockIdx.x / G::C;
     const uint32_t j0 = cluster * a.jobs_per_cluster;
     const uint32_t j1 = min(j0 + a.jobs_per_cluster, a.jobs);
-    SplitCtx<G::C, Sub> ctx;
+    SplitCtx<G::C, Sub, Comp> ctx;
     ctx.smem = smem;
     ctx.stage = nullptr;
     ctx.smem_sa = (uint32_t)__cvta_generic_to_shared(smem);
@@ -250,7 +254,7 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) split_kernel(FusedA
         const uint32_t limb = map_limb(a, jl);
         ctx.o[0] = a.data + (size_t)poly * a.poly_stride + ((size_t)limb << G::LOGN);
         ctx.g[0] = ctx.o[0];
-        ctx.twp = a.tw + ((size_t)limb << G::LOGN);
+        ctx.twp = a.tw + (size_t)limb * kTwStride;
         ctx.q = __ldg(a.q + limb);
         ctx.q2 = 2u * ctx.q;
         ctx.scale_c = a.scale ? __ldg(a.scale + limb) % ctx.q : kNoScale;

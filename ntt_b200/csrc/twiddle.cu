@@ -32,31 +32,51 @@ __device__ __forceinline__ uint32_t dev_brev(uint32_t v, int width) {
     return __brev(v) >> (32 - width);
 }
 
+// base^e mod q by Montgomery square-and-multiply (q < 2^31), normal domain.
+__device__ uint32_t gen_pow(const TwGenLimb& L, uint32_t e) {
+    uint32_t x = dev_redc((uint64_t)L.base * L.r2, L.q, L.nqinv);  // base * R
+    uint32_t acc = L.r_mod;                                          // 1 * R
+    while (e) {
+        if (e & 1u) acc = dev_redc((uint64_t)acc * x, L.q, L.nqinv);
+        x = dev_redc((uint64_t)x * x, L.q, L.nqinv);
+        e >>= 1;
+    }
+    return dev_redc(acc, L.q, L.nqinv);  // leave the Montgomery domain
+}
+
 // One thread per table entry; blockIdx.y = limb.
 __global__ void twiddle_gen_kernel(TwPair* out, const TwGenLimb* limbs, int logN) {
     const uint32_t N = 1u << logN;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const TwGenLimb L = limbs[blockIdx.y];
-    uint32_t w;
-    if (i == 0) {
-        w = L.fold0;
-    } else if (i == 1) {
-        w = L.fold1;
-    } else {
-        // base^bitrev(i) by Montgomery square-and-multiply (q < 2^31)
-        uint32_t e = dev_brev(i, logN);
-        uint32_t x = dev_redc((uint64_t)L.base * L.r2, L.q, L.nqinv);  // base * R
-        uint32_t acc = L.r_mod;                                          // 1 * R
-        while (e) {
-            if (e & 1u) acc = dev_redc((uint64_t)acc * x, L.q, L.nqinv);
-            x = dev_redc((uint64_t)x * x, L.q, L.nqinv);
-            e >>= 1;
-        }
-        w = dev_redc(acc, L.q, L.nqinv);  // leave the Montgomery domain
-    }
+    const uint32_t w = i == 0 ? L.fold0 : i == 1 ? L.fold1 : gen_pow(L, dev_brev(i, logN));
     out[(size_t)blockIdx.y * N + tw_slot(i, logN)] =
         TwPair{w, (uint32_t)(((uint64_t)w << 32) / L.q)};
+}
+
+// Compressed tables (arith.cuh, tw_comp_*): one thread per slot of
+// tw_comp_entries(logN) per limb.  Slots below N/16 hold entries 0 .. N/16-1
+// (the folded 0 and 1 included), then four base blocks of N/32 entries
+// (stages logN-4 .. logN-1: entry H + m F), then the 16 unit-step factors
+// base^bitrev(c), factor 0 = 1, never folded.
+__global__ void twiddle_gen_comp_kernel(TwPair* out, const TwGenLimb* limbs, int logN) {
+    const uint32_t N = 1u << logN, S = N >> 5, E = tw_comp_entries(logN);
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= E) return;
+    const TwGenLimb L = limbs[blockIdx.y];
+    uint32_t w;
+    if (k >= 6 * S) {
+        w = gen_pow(L, dev_brev(k - 6 * S, logN));
+    } else {
+        uint32_t i = k;
+        if (k >= 2 * S) {
+            const uint32_t b = (k - 2 * S) / S, m = (k - 2 * S) % S;  // block b: p = 3 - b
+            i = (N >> (4 - b)) + m * (2u << b);
+        }
+        w = i == 0 ? L.fold0 : i == 1 ? L.fold1 : gen_pow(L, dev_brev(i, logN));
+    }
+    out[(size_t)blockIdx.y * E + k] = TwPair{w, (uint32_t)(((uint64_t)w << 32) / L.q)};
 }
 
 // Import the reference's Montgomery-form tables (tw_mont[i] = to_mont(w_i)).
@@ -146,6 +166,14 @@ cudaError_t launch_twiddle_gen(TwPair* out, const TwGenLimb* limbs_dev, int limb
     const uint32_t N = 1u << logN;
     dim3 block(N < 256 ? N : 256), grid((N + block.x - 1) / block.x, limbs);
     twiddle_gen_kernel<<<grid, block, 0, s>>>(out, limbs_dev, logN);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_twiddle_gen_comp(TwPair* out, const TwGenLimb* limbs_dev, int limbs, int logN,
+                                    cudaStream_t s) {
+    const uint32_t E = tw_comp_entries(logN);
+    dim3 block(256), grid((E + 255) / 256, limbs);
+    twiddle_gen_comp_kernel<<<grid, block, 0, s>>>(out, limbs_dev, logN);
     return cudaGetLastError();
 }
 

@@ -19,6 +19,10 @@ struct TwGenLimb {
 
 cudaError_t launch_twiddle_gen(TwPair* out, const TwGenLimb* limbs_dev, int limbs, int logN,
                                cudaStream_t s);
+// Compressed tables (arith.cuh, tw_comp_*): tw_comp_entries(logN) pairs per
+// limb, logN >= kTwCompMinLogN.
+cudaError_t launch_twiddle_gen_comp(TwPair* out, const TwGenLimb* limbs_dev, int limbs, int logN,
+                                    cudaStream_t s);
 cudaError_t launch_twiddle_import(TwPair* out, const uint32_t* tw_mont, const uint32_t* moduli,
                                   const uint32_t* nqinv, const uint32_t* aux, int limbs,
                                   int logN, int inverse, cudaStream_t s);
