@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-multiply", action="store_true")
     ap.add_argument("--multiply-steps", type=int, default=10)
     ap.add_argument("--no-compressed", action="store_true")
+    ap.add_argument("--no-small", action="store_true")
     ap.add_argument("--compressed-steps", type=int, default=50)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=20000)
@@ -427,6 +428,8 @@ def run_ours(args):
         out["fused_multiply"] = bench_multiply(args, torch, nb, stream)
     if not args.no_compressed:
         out["compressed_twiddles"] = bench_compressed(args, torch, nb, stream, d, P)
+    if not args.no_small:
+        out["small_sizes"] = bench_small(args, torch, nb, stream)
     if not args.no_serve:
         out["serve"] = bench_serve(args, torch, nb)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -460,6 +463,11 @@ def summary(out):
         fm = out["fused_multiply"]
         s["multiply_speedup_vs_unfused"] = r(fm["speedup_vs_unfused"])
         s["multiply_batch_tiles_speedup_vs_unfused"] = r(fm["batch_tiles"]["speedup_vs_unfused"])
+        s["multiply_spectrum_speedup_vs_unfused"] = r(fm["spectrum"]["speedup_vs_unfused"])
+    if "small_sizes" in out:
+        s["small_warp_speedup_vs_shared"] = {k: r(v["speedup_vs_shared"])
+                                             for k, v in out["small_sizes"].items()
+                                             if isinstance(v, dict)}
     if "compressed_twiddles" in out:
         ct = out["compressed_twiddles"]
         s["compressed_headline_ratio"] = r(ct["headline"]["speedup_vs_full"])
@@ -478,6 +486,46 @@ def summary(out):
 
 
 RAGGED = dict(seed=SEED, count=256, logn=tuple(range(12, 17)), limbs=(1, 48), bits=(30,))
+
+
+def bench_small(args, torch, nb, stream):
+    """Small limbs (logN 6 and 9, 16 limbs of 30-bit primes, 2048
+    polynomials = 8 / 64 MiB), step = forward + inverse, CUDA events: the
+    warp-per-limb kernel (registers, the last five stages through shfl.xor)
+    against the shared-memory kernel (a CTA per limb, one shared-memory round
+    and one barrier per stage).  Same words (checked)."""
+    from ntt_b200 import mixes
+    sh = stream.cuda_stream
+    res = {}
+    for logN in (6, 9):
+        limbs, polys = 16, 2048
+        mods = list(mixes.prime_pool(logN, 30, limbs))
+        job = mixes.MixJob(nb.OP_FORWARD, logN, mods)
+        g = torch.Generator(device="cuda")
+        g.manual_seed(SEED + logN)
+        x = torch.stack([mixes.uniform_device(torch, job, g) for _ in range(polys)])
+        pw, ps = nb.Plan(logN, mods), nb.Plan(logN, mods)
+        ps.set_small_kernel(nb.SMALL_SHARED)
+        y = x.clone()
+        with torch.cuda.stream(stream):
+            pw.forward_many(x, polys, 0, sh)
+            ps.forward_many(y, polys, 0, sh)
+        stream.synchronize()
+        if not torch.equal(x, y):
+            raise RuntimeError("warp and shared-memory kernels differ")
+        del y
+
+        def step(p):
+            return lambda: (p.forward_many(x, polys, 0, sh), p.inverse_many(x, polys, 0, sh))
+        t_w = device_time(torch, stream, step(pw), 50, 5)
+        t_s = device_time(torch, stream, step(ps), 50, 5)
+        res[f"logN{logN}"] = {
+            "workload": f"{polys} x 2^{logN} x {limbs} limbs, forward + inverse",
+            "warp_ms": t_w, "shared_ms": t_s, "speedup_vs_shared": t_s / t_w,
+            "warp_limb_ntt_per_s": 2 * polys * limbs / (t_w / 1000.0)}
+        pw.close()
+        ps.close()
+    return res
 
 
 def bench_compressed(args, torch, nb, stream, d, P):
@@ -702,7 +750,31 @@ def bench_multiply(args, torch, nb, stream):
         p.pointwise_mul(tb, ta, tb, pairs, 0, sh)
         p.inverse_many(tb, pairs, 0, sh)
 
+    # the product with a resident spectrum (a transformed once, outside the
+    # timed region): two launches on split plans against forward, pointwise,
+    # inverse
+    spec = a.clone()
+    with torch.cuda.stream(stream):
+        p.forward_many(spec, pairs, 0, sh)
+        sb, su = b.clone(), b.clone()
+        p.multiply_spectrum_many(spec, sb, pairs, 0, sh)
+        p.forward_many(su, pairs, 0, sh)
+        p.pointwise_mul(su, spec, su, pairs, 0, sh)
+        p.inverse_many(su, pairs, 0, sh)
+    stream.synchronize()
+    if not torch.equal(sb, su):
+        raise RuntimeError("spectrum product and its unfused form differ")
+
+    def spec_unfused():
+        p.forward_many(su, pairs, 0, sh)
+        p.pointwise_mul(su, spec, su, pairs, 0, sh)
+        p.inverse_many(su, pairs, 0, sh)
+
     w = 3
+    spec_ms = device_time(torch, stream, lambda: p.multiply_spectrum_many(spec, sb, pairs, 0, sh),
+                          args.multiply_steps, w)
+    spec_unfused_ms = device_time(torch, stream, spec_unfused, args.multiply_steps, w)
+    del su
     fused_ms = device_time(torch, stream, lambda: p.multiply_many(a, pb, pairs, 0, sh),
                            args.multiply_steps, w)
     unfused_ms = device_time(torch, stream, unfused, args.multiply_steps, w)
@@ -722,6 +794,12 @@ def bench_multiply(args, torch, nb, stream):
         "unfused": {"value": products / (unfused_ms / 1000.0), "ms_per_step": unfused_ms,
                     "launches_per_step": 4, "algorithmic_bytes": 36 * words},
         "speedup_vs_unfused": unfused_ms / fused_ms,
+        "spectrum": {"form": "ntt_multiply_spectrum_many with NTT(a) resident: forward of b "
+                             "with the product on its final store, inverse (2 launches)",
+                     "value": products / (spec_ms / 1000.0), "ms_per_step": spec_ms,
+                     "launches_per_step": 2, "unfused_ms": spec_unfused_ms,
+                     "unfused_form": "forward(b), pointwise_mul, inverse(b) (3 launches)",
+                     "speedup_vs_unfused": spec_unfused_ms / spec_ms},
         "batch_tiles": {"value": products / (tiles_ms / 1000.0), "ms_per_step": tiles_ms,
                         "launches_per_step": 1, "speedup_vs_unfused": unfused_ms / tiles_ms,
                         "cluster_ctas": tiles.info.cluster_ctas, "clusters": tiles.info.clusters},

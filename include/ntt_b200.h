@@ -261,6 +261,19 @@ NTT_API ntt_status_t ntt_pointwise_mul(const ntt_plan_t* plan, uint32_t* c_dev,
 NTT_API ntt_status_t ntt_multiply_many(const ntt_plan_t* plan, const uint32_t* a_dev,
                                        uint32_t* b_dev, size_t polys, size_t poly_stride,
                                        ntt_stream_t stream);
+/* b <- INTT(NTT(b) (.) a_spec) per limb: the negacyclic product of each b
+ * with a polynomial whose spectrum a_spec (the plan's forward output:
+ * Montgomery domain, bit-reversed, canonical) is already resident -- the
+ * plaintext-times-ciphertext pattern of RNS schemes, where one operand is
+ * transformed once and used many times.  Split plans (logN 15..17) run two
+ * launches: the forward of b with the Montgomery product by the spectrum word
+ * on its final store, then the inverse; other plans run forward,
+ * ntt_pointwise_mul and inverse.  a_spec has b's shape and stride, is only
+ * read and must not overlap b; 16-byte aligned.  No reference counterpart
+ * (the reference has no multiply). */
+NTT_API ntt_status_t ntt_multiply_spectrum_many(const ntt_plan_t* plan, const uint32_t* a_spec_dev,
+                                                uint32_t* b_dev, size_t polys, size_t poly_stride,
+                                                ntt_stream_t stream);
 /* Diagnostic (no reference counterpart): 32-bit integer multiplies per second
  * the current device sustains on the transforms' multiply mix (Shoup
  * products: one multiply-high and two multiply-lows each), measured by a

@@ -63,6 +63,14 @@ NTT_API ntt_status_t ntt_plan_force_config(ntt_plan_t* plan, int fwd_index, int 
 /* Work distribution of the plan's launches (NTT_SCHEDULE_*; default
  * NTT_SCHEDULE_DIRECT). */
 NTT_API ntt_status_t ntt_plan_set_schedule(ntt_plan_t* plan, int schedule);
+/* Kernel of the plan's launches at logN 6..9 (results identical):
+ * NTT_SMALL_WARP (default): a warp per limb, the limb in registers, the last
+ *   five stages pairing lanes through shfl.xor;
+ * NTT_SMALL_SHARED: a CTA per limb, one shared-memory round and one barrier
+ *   per stage (the path of logN 1..5). */
+#define NTT_SMALL_WARP 0
+#define NTT_SMALL_SHARED 1
+NTT_API ntt_status_t ntt_plan_set_small_kernel(ntt_plan_t* plan, int kind);
 /* Self-test of the kernels' failure detection (no reference counterpart):
  * runs, on `stream`, the bounded mbarrier wait the transform kernels use,
  * on a barrier that nothing ever completes, with a limit of `limit` tries

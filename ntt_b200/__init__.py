@@ -100,6 +100,7 @@ class TuneResult(ctypes.Structure):
 
 NTT_OK = 0
 PLAN_COMPRESSED_TWIDDLES = 1  # include/ntt_b200.h: NTT_PLAN_COMPRESSED_TWIDDLES
+SMALL_WARP, SMALL_SHARED = 0, 1  # include/ntt_b200_tune.h: NTT_SMALL_*
 STATUS_NAMES = {
     0: "NTT_OK", 1: "NTT_ERR_INVALID_ARGUMENT", 2: "NTT_ERR_MODULUS", 3: "NTT_ERR_ROOT",
     4: "NTT_ERR_MODULUS_RANGE", 5: "NTT_ERR_UNSUPPORTED", 6: "NTT_ERR_MISALIGNED",
@@ -153,6 +154,7 @@ _sig("ntt_forward_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_inverse_many", _st, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_pointwise_mul", _st, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_multiply_many", _st, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
+_sig("ntt_multiply_spectrum_many", _st, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _vp)
 _sig("ntt_measure_int_peak", _st, ctypes.POINTER(ctypes.c_double))
 _sig("ntt_launch_ntt", _st, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_int,
      ctypes.POINTER(PhaseConfig), ctypes.POINTER(PhaseConfig))
@@ -167,6 +169,7 @@ _sig("ntt_autotune", _st, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int
 _sig("ntt_autotune_forget", None)
 _sig("ntt_plan_force_config", _st, _vp, ctypes.c_int, ctypes.c_int)
 _sig("ntt_plan_set_schedule", _st, _vp, ctypes.c_int)
+_sig("ntt_plan_set_small_kernel", _st, _vp, ctypes.c_int)
 _sig("ntt_plan_check", _st, _vp, ctypes.POINTER(ctypes.c_uint32))
 _sig("ntt_config_resident_clusters", ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
 SCHEDULE_DIRECT = 0
@@ -322,6 +325,11 @@ class Plan:
         """Pin the plan to compiled configurations (see kernel_configs())."""
         _check(_lib.ntt_plan_force_config(self._h, fwd_index, inv_index), "ntt_plan_force_config")
 
+    def set_small_kernel(self, kind: int = SMALL_WARP):
+        """logN 6..9: SMALL_WARP (a warp per limb, shuffles) or SMALL_SHARED
+        (a CTA per limb, a shared-memory round per stage)."""
+        _check(_lib.ntt_plan_set_small_kernel(self._h, kind), "ntt_plan_set_small_kernel")
+
     def set_schedule(self, schedule: int = SCHEDULE_DIRECT):
         """SCHEDULE_DIRECT: one limb per cluster, input from global memory;
         SCHEDULE_STAGED: resident clusters with the next input slab
@@ -404,6 +412,13 @@ class Plan:
         """c = a (.) b: Montgomery product of two forward outputs per limb."""
         _check(_lib.ntt_pointwise_mul(self._h, _ptr(c), _ptr(a), _ptr(b), polys, poly_stride,
                                       _stream(stream)), "ntt_pointwise_mul")
+
+    def multiply_spectrum_many(self, a_spec, b, polys: int = 1, poly_stride: int = 0,
+                               stream=None):
+        """b <- INTT(NTT(b) (.) a_spec): the product with an operand whose
+        spectrum (this plan's forward output) is already resident."""
+        _check(_lib.ntt_multiply_spectrum_many(self._h, _ptr(a_spec), _ptr(b), polys, poly_stride,
+                                               _stream(stream)), "ntt_multiply_spectrum_many")
 
     def multiply_many(self, a, b, polys: int = 1, poly_stride: int = 0, stream=None):
         """b <- a * b negacyclic per limb (normal domain), a read only: three

@@ -178,11 +178,15 @@ static uint32_t smem_of(const FusedConfig* c, int schedule) {
 }
 
 static const void* kernel_of(const FusedConfig* c, bool fwd, int schedule, bool lazy2,
-                             bool mul = false, bool sub = false, bool comp = false) {
-    if (mul) return c->kern_mul[lazy2 ? 1 : 0];
-    if (sub) return c->kern_sub[lazy2 ? 1 : 0];
-    if (comp) return c->kern_comp[fwd ? 1 : 0][lazy2 ? 1 : 0];
-    return c->kernel(schedule == NTT_SCHEDULE_STAGED, fwd, lazy2);
+                             KernelVariant v = KernelVariant::Plain) {
+    const int l2 = lazy2 ? 1 : 0;
+    switch (v) {
+        case KernelVariant::Mul: return c->kern_mul[l2];
+        case KernelVariant::SubScale: return c->kern_sub[l2];
+        case KernelVariant::Compressed: return c->kern_comp[fwd ? 1 : 0][l2];
+        case KernelVariant::MulSpec: return c->kern_mulspec[l2];
+        default: return c->kernel(schedule == NTT_SCHEDULE_STAGED, fwd, lazy2);
+    }
 }
 
 ntt_status_t prepare_function(const FusedConfig* c, const void* fn, int schedule) {
@@ -253,11 +257,11 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule) {
 // wave of resident clusters, each running a contiguous chunk of limb-major
 // jobs with the next input slab bulk-copied ahead.
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
-                          int schedule, bool lazy2, bool mul, bool sub, bool comp) {
+                          int schedule, bool lazy2, KernelVariant v) {
     if (a.jobs == 0) return NTT_OK;
-    // the output epilogues and the split kernels have a direct form only
-    if (mul || sub || c->split) schedule = NTT_SCHEDULE_DIRECT;
-    const void* fn = kernel_of(c, fwd, schedule, lazy2, mul, sub, comp);
+    // the variants and the split kernels have a direct form only
+    if (v != KernelVariant::Plain || c->split) schedule = NTT_SCHEDULE_DIRECT;
+    const void* fn = kernel_of(c, fwd, schedule, lazy2, v);
     if (!fn) return fail(NTT_ERR_UNSUPPORTED, "configuration has no such kernel");
     ntt_status_t st = prepare_function(c, fn, schedule);
     if (st != NTT_OK) return st;
@@ -316,6 +320,7 @@ struct ntt_plan {
     int schedule = NTT_SCHEDULE_DIRECT;
     bool lazy2 = false;  // a modulus >= 2^30: every limb uses the [0, 2q) discipline
     bool compressed = false;  // compressed twiddle tables (split configurations only)
+    bool small_shared = false;  // logN 6..9: the shared-memory kernel instead of the warp one
     size_t tw_stride = 0;     // table pairs per limb: N, or tw_comp_entries(logN)
 };
 
@@ -654,6 +659,14 @@ ntt_status_t ntt_selftest_wait_expiry(const ntt_plan_t* p, uint32_t limit, ntt_s
     return NTT_OK;
 }
 
+ntt_status_t ntt_plan_set_small_kernel(ntt_plan_t* p, int kind) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    if (kind != NTT_SMALL_WARP && kind != NTT_SMALL_SHARED)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "unknown small-size kernel %d", kind);
+    p->small_shared = kind == NTT_SMALL_SHARED;
+    return NTT_OK;
+}
+
 ntt_status_t ntt_plan_set_schedule(ntt_plan_t* p, int schedule) {
     if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
     if (schedule != NTT_SCHEDULE_DIRECT && schedule != NTT_SCHEDULE_STAGED)
@@ -684,12 +697,16 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
                            const uint32_t* mul_src, const uint32_t* scale, const LimbOps* ops) {
     static const LimbOps kNone{};
     if (!ops) ops = &kNone;
-    const bool sub = ops->sub != nullptr;
-    if (ops->compressed && (mul_src || sub))
+    const bool sub = ops->sub != nullptr, mulspec = ops->spec != nullptr;
+    if (ops->compressed && (mul_src || sub || mulspec))
         return fail(NTT_ERR_UNSUPPORTED,
                     "plans with compressed twiddle tables run plain and scaled transforms only");
     if (ops->compressed && (!cfg || !cfg->kern_comp[0][0]))
         return fail(NTT_ERR_UNSUPPORTED, "no compressed-table kernel for this configuration");
+    if (mulspec && (!fwd || mul_src || sub || !cfg || !cfg->kern_mulspec[0]))
+        return fail(NTT_ERR_UNSUPPORTED, "the spectrum product runs on split forwards only");
+    if (mulspec && ((((uintptr_t)ops->spec & 15u) != 0) || (polys > 1 && (ops->spec_stride & 3u) != 0)))
+        return fail(NTT_ERR_MISALIGNED, "spectrum must be 16-byte aligned (stride a multiple of 4 words)");
     if (polys == 0 || limbs == 0) return NTT_OK;
     if (!a) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL data pointer");
     if (sub && (!fwd || mul_src))
@@ -725,14 +742,21 @@ ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, c
                      (unsigned long long)stride, status, mul_src, (unsigned long long)stride,
                      scale, ops->skip_at, ops->skip_len, ops->sub,
                      (unsigned long long)ops->sub_stride, ops->sub_begin, ops->sub_end,
-                     ops->sub_mul};
-        return launch_fused(cfg, fwd, fa, s, schedule, lazy2, mul_src != nullptr, sub,
-                            ops->compressed);
+                     ops->sub_mul, ops->spec, (unsigned long long)ops->spec_stride};
+        const KernelVariant v = mul_src ? KernelVariant::Mul
+                                : sub ? KernelVariant::SubScale
+                                : mulspec ? KernelVariant::MulSpec
+                                : ops->compressed ? KernelVariant::Compressed
+                                : KernelVariant::Plain;
+        return launch_fused(cfg, fwd, fa, s, schedule, lazy2, v);
     }
     SmallArgs sa{a, tw, q, (uint32_t)limbs, (uint32_t)jobs, (unsigned long long)stride, logN,
                  scale, ops->skip_at, ops->skip_len, ops->sub,
                  (unsigned long long)ops->sub_stride, ops->sub_begin, ops->sub_end, ops->sub_mul};
-    NTT_CUDA_TRY(launch_small(sa, fwd, s), "small NTT launch");
+    if (logN >= kWarpMinLogN && !ops->small_shared)
+        NTT_CUDA_TRY(launch_warp(sa, fwd, s), "warp NTT launch");
+    else
+        NTT_CUDA_TRY(launch_small(sa, fwd, s), "small NTT launch");
     return NTT_OK;
 }
 
@@ -755,6 +779,7 @@ static ntt_status_t plan_run(const ntt_plan_t* p, uint32_t* a, size_t polys, siz
     int launch_limbs = limb_end - limb_begin;
     LimbOps o = ops ? *ops : LimbOps{};
     o.compressed = p->compressed;
+    o.small_shared = p->small_shared;
     launch_limbs -= (int)o.skip_len;
     return run_transform(p->logN, cfg, (fwd ? p->fwd : p->inv) + (size_t)limb_begin * p->tw_stride,
                          p->q + limb_begin, launch_limbs, a ? a + off : nullptr, polys, stride,
@@ -908,6 +933,34 @@ static ntt_status_t launch_split_mul(const FusedConfig* c, const ntt_plan_t* p, 
     void* args[] = {&arg};
     NTT_CUDA_TRY(cudaLaunchKernelExC(&lc, fn, args), "split multiply launch");
     return NTT_OK;
+}
+
+ntt_status_t ntt_multiply_spectrum_many(const ntt_plan_t* p, const uint32_t* a_spec, uint32_t* b,
+                                        size_t polys, size_t stride, ntt_stream_t s) {
+    if (!p || !a_spec || !b) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (stride == 0) stride = (size_t)p->limbs << p->logN;
+    if (polys == 0) return NTT_OK;
+    if (polys > 1 && stride < ((size_t)p->limbs << p->logN))
+        return fail(NTT_ERR_INVALID_ARGUMENT, "poly_stride smaller than limbs * N");
+    const size_t span = 4 * extent_words(polys, stride, p->limbs, p->logN);
+    if ((uintptr_t)a_spec < (uintptr_t)b + span && (uintptr_t)b < (uintptr_t)a_spec + span)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "the spectrum must not overlap b");
+    // checked before the first launch, so a refused call leaves b untouched
+    if ((((uintptr_t)a_spec | (uintptr_t)b) & 15u) != 0 || (polys > 1 && (stride & 3u) != 0))
+        return fail(NTT_ERR_MISALIGNED, "data must be 16-byte aligned (stride a multiple of 4 words)");
+    const FusedConfig* cf = p->cfg_fwd;
+    if (cf && (polys == 1 || polys < (size_t)cf->np)) cf = p->cfg_fwd1;
+    if (!p->compressed && cf && cf->kern_mulspec[0]) {
+        // split plans: the product rides on the forward's final store
+        LimbOps o;
+        o.spec = a_spec;
+        o.spec_stride = stride;
+        if (ntt_status_t st = plan_run(p, b, polys, stride, true, s, nullptr, &o)) return st;
+    } else {
+        if (ntt_status_t st = plan_run(p, b, polys, stride, true, s)) return st;
+        if (ntt_status_t st = ntt_pointwise_mul(p, b, b, a_spec, polys, stride, s)) return st;
+    }
+    return plan_run(p, b, polys, stride, false, s);
 }
 
 ntt_status_t ntt_multiply_many(const ntt_plan_t* p, const uint32_t* a, uint32_t* b,

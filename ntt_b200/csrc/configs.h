@@ -39,7 +39,7 @@
 //   back to global memory; the limb's CTAs then exchange through L2 (in
 //   place) across one cluster barrier; phase 2 = passes of K2A, K2B and
 //   LOGN - EB - K2A - K2B (if nonzero) stages over the CTA's contiguous rows.
-#define NTTB_SPLIT_N16(S) S(16, 3, 5, 4, 4) S(16, 3, 4, 4, 4)
+#define NTTB_SPLIT_N16(S) S(16, 3, 5, 4, 4) S(16, 3, 4, 4, 4) S(16, 3, 5, 3, 4)
 #define NTTB_SPLIT_REST(S) S(17, 4, 5, 4, 4) S(15, 2, 5, 5, 5) S(15, 2, 4, 4, 4)
 #define NTTB_SPLIT_ALL(S) NTTB_SPLIT_N16(S) NTTB_SPLIT_REST(S)
 
@@ -72,6 +72,9 @@ struct FusedConfig {
     // with NTT_PLAN_COMPRESSED_TWIDDLES) [fwd][lazy2]; null for cluster
     // configurations
     const void* kern_comp[2][2];
+    // split: the forward whose final store multiplies by a resident spectrum
+    // (ntt_multiply_spectrum_many) [lazy2]; null for cluster configurations
+    const void* kern_mulspec[2];
     bool has_mul() const { return kern_mul[0] != nullptr; }
     const void* kernel(bool staged, bool fwd, bool lazy2) const {
         return kern[staged ? 1 : 0][fwd ? 1 : 0][lazy2 ? 1 : 0];

@@ -48,7 +48,18 @@ struct FusedArgs {
     unsigned long long sub_stride;
     uint32_t sub_begin, sub_end;
     const uint32_t* sub_mul;
+    // spectrum-product output (split forwards, Out == kOutMulSpec): the
+    // final store writes the Montgomery product of y with the word at the
+    // same place of spec[poly * spec_stride + limb * N] (another forward's
+    // output, read once)
+    const uint32_t* spec;
+    unsigned long long spec_stride;
 };
+
+// Output modes of the transform kernels' final store.
+constexpr int kOutPlain = 0;
+constexpr int kOutSubScale = 1;  // y - e s (ModDown)
+constexpr int kOutMulSpec = 2;   // mont_mul(y, s) (product with a resident spectrum)
 
 __device__ __forceinline__ uint32_t map_limb(const FusedArgs& a, uint32_t l) {
     return l >= a.skip_at ? l + a.skip_len : l;
@@ -169,14 +180,16 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst_sa, const void* src, uint3
 // Memory interface used by the pass code (ntt_core.cuh): every access is a
 // per-thread base plus a compile-time offset, which the compiler turns into
 // an immediate address offset.
-template <int C, bool Staged, int NP, bool Mul = false, bool Sub = false>
+// Out (kOut*): the final store's output mode; SubOut carries the word it
+// reads (subtrahend or spectrum).
+template <int C, bool Staged, int NP, bool Mul = false, int Out = kOutPlain>
 struct DevCtx {
     static constexpr bool kStaged = Staged;
-    static constexpr bool kSub = Sub;
+    static constexpr bool kSub = Out != kOutPlain;
     uint32_t* g[NP];  // limb base of each polynomial of the job (input)
     uint32_t* o[NP];  // ... output (the input's place, or the spectrum for Mul)
-    const uint32_t* sb[NP];  // Sub: the subtrahend's limb base (nullptr: none)
-    TwPair sub_e;            // Sub: e and its Shoup companion
+    const uint32_t* sb[NP];  // Out: the subtrahend's / spectrum's limb base (nullptr: none)
+    TwPair sub_e;            // kOutSubScale: e and its Shoup companion
     uint32_t qinv;    // Mul: -q^{-1} mod 2^32
     uint32_t live;    // Mul: bit p set when slot p is not a repeated polynomial
     const TwPair* __restrict__ twp;
@@ -204,22 +217,27 @@ struct DevCtx {
     // word at the output's place (written by an earlier launch: read via L2)
     __device__ __forceinline__ auto o_base(int p, uint32_t off) const {
         if constexpr (Mul) return MulOut{o[p] + off, ((live >> p) & 1u) != 0};
-        else if constexpr (Sub) return SubOut{o[p] + off, sb[p] ? sb[p] + off : nullptr};
+        else if constexpr (Out != kOutPlain) return SubOut{o[p] + off, sb[p] ? sb[p] + off : nullptr};
         else return o[p] + off;
     }
-    // Sub: y - e * s with the subtrahend word at the output's place (read
-    // once: streamed)
+    // kOutSubScale: y - e * s; kOutMulSpec: the Montgomery product y * s;
+    // s the word at the output's place of the second operand (read once:
+    // streamed)
+    __device__ __forceinline__ uint32_t out_word(uint32_t v, uint32_t s) const {
+        if constexpr (Out == kOutMulSpec) return mont_mul(v, s, q, qinv);
+        else return sub_scaled(v, s, sub_e, q);
+    }
     __device__ __forceinline__ void o_st(SubOut b, uint32_t c, uint32_t v) const {
-        b.p[c] = b.s ? sub_scaled(v, __ldcs(b.s + c), sub_e, q) : v;
+        b.p[c] = b.s ? out_word(v, __ldcs(b.s + c)) : v;
     }
     __device__ __forceinline__ void o_st4(SubOut b, uint32_t c, uint32_t x, uint32_t y,
                                           uint32_t z, uint32_t w) const {
         if (b.s) {
             const uint4 k = __ldcs(reinterpret_cast<const uint4*>(b.s + c));
-            x = sub_scaled(x, k.x, sub_e, q);
-            y = sub_scaled(y, k.y, sub_e, q);
-            z = sub_scaled(z, k.z, sub_e, q);
-            w = sub_scaled(w, k.w, sub_e, q);
+            x = out_word(x, k.x);
+            y = out_word(y, k.y);
+            z = out_word(z, k.z);
+            w = out_word(w, k.w);
         }
         *reinterpret_cast<uint4*>(b.p + c) = make_uint4(x, y, z, w);
     }
@@ -435,7 +453,7 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedA
         if (j0 < j1) issue_slab<G, Fwd>(a, j0, rank, stage_sa, mbar_sa);
     }
     static_assert(!Staged || G::NP == 1, "the staged schedule carries one polynomial per job");
-    DevCtx<G::C, Staged, G::NP, Mul, Sub> ctx;
+    DevCtx<G::C, Staged, G::NP, Mul, Sub ? kOutSubScale : kOutPlain> ctx;
     const uint32_t groups = (a.polys + G::NP - 1) / G::NP;
     ctx.smem = smem;
     ctx.stage = smem + G::STAGE_OFF_WORDS;

@@ -228,6 +228,14 @@ struct SplitLayoutTable<16, 3, 4, 4, 4> {
 };
 
 template <>
+struct SplitLayoutTable<16, 3, 5, 3, 4> {
+    static constexpr int XW[5] = {5, 4, 8, 16, 9708};
+    static constexpr uint32_t lanes_P2A = 0x1fu;
+    static constexpr uint32_t lanes_P2B = 0x30eu;
+    static constexpr uint32_t lanes_P2C = 0x3e0u;
+};
+
+template <>
 struct SplitLayoutTable<17, 4, 5, 4, 4> {
     static constexpr int XW[5] = {5, 4, 8, 16, 9708};
     static constexpr uint32_t lanes_P2A = 0x1fu;

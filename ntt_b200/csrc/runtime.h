@@ -29,11 +29,14 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule);
 // One launch of a fused configuration under a schedule (NTT_SCHEDULE_*);
 // lazy2: some modulus is >= 2^30 (the [0, 2q) range discipline for all).
 // mul: the direct forward with the product epilogue (FusedArgs.src).
-// sub: the direct forward with the subtract-and-scale output (FusedArgs.sub).
-// comp: the kernels over compressed twiddle tables (split configurations).
+// Kernel variants of a configuration (FusedConfig's kern_* entries): the
+// plain transforms; the direct forward with the product epilogue
+// (FusedArgs.src), with the subtract-and-scale output (FusedArgs.sub), with
+// the product by a resident spectrum (FusedArgs.spec); the transforms over
+// compressed twiddle tables.
+enum class KernelVariant { Plain, Mul, SubScale, MulSpec, Compressed };
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
-                          int schedule, bool lazy2, bool mul = false, bool sub = false,
-                          bool comp = false);
+                          int schedule, bool lazy2, KernelVariant v = KernelVariant::Plain);
 ntt_status_t validate_modulus(int logN, ModulusConfig m, ModulusRuntime* rt);
 // Validates m and fills the twiddle-generation inputs of both directions
 // (entries 0/1 carry the folded Montgomery / N^{-1} R^{-1} factors).
@@ -46,9 +49,9 @@ ntt_status_t twiddle_gen_inputs(int logN, ModulusConfig m, TwGenLimb* fwd, TwGen
 // scale (optional, device, one constant per limb): forward of c * x, or
 // c * inverse, folded into the limb's stage 0.
 // ops (optional): the limb map and the subtract-and-scale output of the
-// ModUp / ModDown forwards (FusedArgs), and whether `tw` is a compressed
-// table (tw_comp_* layout); `limbs` counts the launch's limbs (the table's
-// limbs minus skip_len).
+// ModUp / ModDown forwards (FusedArgs), the spectrum of the spectrum
+// product, and whether `tw` is a compressed table (tw_comp_* layout);
+// `limbs` counts the launch's limbs (the table's limbs minus skip_len).
 struct LimbOps {
     uint32_t skip_at = 0, skip_len = 0;
     const uint32_t* sub = nullptr;
@@ -56,6 +59,9 @@ struct LimbOps {
     uint32_t sub_begin = 0, sub_end = 0;
     const uint32_t* sub_mul = nullptr;
     bool compressed = false;
+    const uint32_t* spec = nullptr;  // the spectrum the forward's output is multiplied by
+    size_t spec_stride = 0;
+    bool small_shared = false;  // logN 6..9: the shared-memory kernel, not the warp one
 };
 ntt_status_t run_transform(int logN, const FusedConfig* cfg, const TwPair* tw, const uint32_t* q,
                            int limbs, uint32_t* a, size_t polys, size_t stride, bool fwd,

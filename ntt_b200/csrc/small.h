@@ -22,4 +22,8 @@ struct SmallArgs {
     const uint32_t* sub_mul;
 };
 cudaError_t launch_small(const SmallArgs& a, bool fwd, cudaStream_t s);
+// Warp-per-limb kernel (warp.cu) for kWarpMinLogN <= logN <= kSmallMaxLogN:
+// registers and shuffles, same results as launch_small.
+constexpr int kWarpMinLogN = 6;
+cudaError_t launch_warp(const SmallArgs& a, bool fwd, cudaStream_t s);
 }  // namespace nttb

@@ -104,11 +104,11 @@ __device__ __forceinline__ void split_sync() {
 // The cluster kernels' device context, with global loads that either stream
 // (phase-1 input, read once) or bypass L1 (words other CTAs of the cluster
 // rewrote after this SM may have cached their lines).
-template <int C, bool Sub = false, bool Comp = false>
-struct SplitCtx : DevCtx<C, false, 1, false, Sub> {
+template <int C, int Out = kOutPlain, bool Comp = false>
+struct SplitCtx : DevCtx<C, false, 1, false, Out> {
     static constexpr bool kCompTw = Comp;  // compressed twiddle tables (arith.cuh)
     bool cg = false;
-    const uint32_t* sb_final = nullptr;  // Sub: the subtrahend, armed for the last store
+    const uint32_t* sb_final = nullptr;  // Out: the second operand, armed for the last store
     __device__ __forceinline__ uint32_t g_ld(const uint32_t* b, uint32_t c) const {
         return cg ? __ldcg(b + c) : __ldca(b + c);
     }
@@ -230,12 +230,13 @@ __device__ __forceinline__ void split_inverse_body(Ctx& ctx) {
 // per job): cluster c runs job c.  The launcher always gives one job per
 // cluster (the hardware schedules the clusters); a loop over several jobs
 // made the compiler keep per-thread addresses live across jobs and spill.
-// Sub (forward only): the subtract-and-scale output of FusedArgs on the
-// final store.  Comp: compressed twiddle tables (tw_comp_entries pairs per
-// limb; the last four stages multiply by two factors).
-template <class G, bool Fwd, class Arith, bool Sub = false, bool Comp = false>
+// Out (forward only): the final store's output mode (kOutSubScale: the
+// subtract-and-scale output of FusedArgs; kOutMulSpec: the product with a
+// resident spectrum).  Comp: compressed twiddle tables (tw_comp_entries
+// pairs per limb; the last four stages multiply by two factors).
+template <class G, bool Fwd, class Arith, int Out = kOutPlain, bool Comp = false>
 __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) split_kernel(FusedArgs a) {
-    static_assert(!Sub || Fwd, "the subtract-and-scale output follows a forward");
+    static_assert(Out == kOutPlain || Fwd, "the output modes follow a forward");
     static_assert(!Comp || G::LOGN >= kTwCompMinLogN, "compressed tables start at logN 15");
     constexpr uint32_t kTwStride = Comp ? tw_comp_entries(G::LOGN) : (1u << G::LOGN);
     extern __shared__ __align__(16) uint32_t smem[];
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) split_kernel(FusedA
     const uint32_t cluster = blockIdx.x / G::C;
     const uint32_t j0 = cluster * a.jobs_per_cluster;
     const uint32_t j1 = min(j0 + a.jobs_per_cluster, a.jobs);
-    SplitCtx<G::C, Sub, Comp> ctx;
+    SplitCtx<G::C, Out, Comp> ctx;
     ctx.smem = smem;
     ctx.stage = nullptr;
     ctx.smem_sa = (uint32_t)__cvta_generic_to_shared(smem);
@@ -259,11 +260,15 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) split_kernel(FusedA
         ctx.q2 = 2u * ctx.q;
         ctx.scale_c = a.scale ? __ldg(a.scale + limb) % ctx.q : kNoScale;
         ctx.cg = false;
-        if constexpr (Sub) {
+        if constexpr (Out == kOutSubScale) {
             const SubJob sj = sub_job<G::LOGN>(a, limb, poly, ctx.q);
             ctx.sb[0] = nullptr;
             ctx.sb_final = sj.base;
             ctx.sub_e = sj.e;
+        } else if constexpr (Out == kOutMulSpec) {
+            ctx.sb[0] = nullptr;
+            ctx.sb_final = a.spec + (size_t)poly * a.spec_stride + ((size_t)limb << G::LOGN);
+            ctx.qinv = neg_qinv_dev(ctx.q);
         }
         if constexpr (Fwd) split_forward_body<G, Arith>(ctx);
         else split_inverse_body<G, Arith>(ctx);

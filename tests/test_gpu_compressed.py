@@ -97,7 +97,8 @@ def test_compressed_transforms_match_oracle(torch_cuda, logN, limbs, bits, polys
         assert np.array_equal(to_host(d1, xs[-1].shape), T.forward_mont(xs[-1]))
         plan.inverse(d1)
         torch.cuda.synchronize()
-        assert np.array_equal(to_host(d1, xs[-1].shape), xs[-1])
+        want1 = xs[-1] % T.q[:, None]  # the planted 0xFFFFFFFF (polys == 1) comes back reduced
+        assert np.array_equal(to_host(d1, xs[-1].shape), want1)
 
 
 def test_compressed_scaled_skip_and_range(torch_cuda):

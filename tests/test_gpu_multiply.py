@@ -123,3 +123,52 @@ def test_multiply_many_errors(torch_cuda, nb, mixes):
         small.multiply_many(y[0], y[1], 1)
     assert e.value.name == "NTT_ERR_UNSUPPORTED"
     small.close()
+
+
+@pytest.mark.parametrize("logN,bits,compressed", [(8, 30, False), (12, 31, False),
+                                                  (15, 30, False), (16, 31, False),
+                                                  (16, 30, True), (17, 30, False)])
+def test_multiply_spectrum_many(torch_cuda, nb, mixes, logN, bits, compressed):
+    """b <- INTT(NTT(b) (.) NTT(a)) with NTT(a) resident: equal to the unfused
+    calls on every kernel family (the split forward's spectrum-product
+    store at logN 15..17, forward + pointwise + inverse elsewhere and on
+    compressed plans); the spectrum is only read."""
+    torch = torch_cuda
+    pairs, limbs = 3, 4
+    mods = list(mixes.prime_pool(logN, bits, limbs))
+    a, b = pair_inputs(torch, mixes, nb, logN, mods, pairs, 40 + logN)
+    p = nb.Plan(logN, mods, compressed_twiddles=compressed)
+    expect = unfused(p, a, b, pairs)
+    spec = a.clone()
+    p.forward_many(spec, pairs)
+    spec_h = host(spec).copy()
+    p.multiply_spectrum_many(spec, b, pairs)
+    torch.cuda.synchronize()
+    assert torch.equal(b, expect)
+    assert np.array_equal(host(spec), spec_h)
+    p.close()
+
+
+def test_multiply_spectrum_schoolbook_and_errors(torch_cuda, nb, mixes):
+    torch = torch_cuda
+    logN, pairs, limbs = 16, 2, 6
+    mods = list(mixes.prime_pool(logN, 30, limbs))
+    a, b = pair_inputs(torch, mixes, nb, logN, mods, pairs, 21)
+    a_h, b_h = host(a).copy(), host(b).copy()
+    p = nb.Plan(logN, mods)
+    spec = a.clone()
+    p.forward_many(spec, pairs)
+    p.multiply_spectrum_many(spec, b, pairs)
+    torch.cuda.synchronize()
+    c = host(b)
+    rng = np.random.default_rng(61)
+    for _ in range(32):
+        i, l, k = int(rng.integers(pairs)), int(rng.integers(limbs)), int(rng.integers(1 << logN))
+        assert int(c[i, l, k]) == O.negacyclic_coeff(a_h[i, l], b_h[i, l], logN, mods[l][0], k)
+    with pytest.raises(nb.NttError) as e:  # the spectrum overlaps b
+        p.multiply_spectrum_many(b, b, 1)
+    assert e.value.name == "NTT_ERR_INVALID_ARGUMENT"
+    with pytest.raises(nb.NttError) as e:
+        p.multiply_spectrum_many(spec.data_ptr() + 4, b, 1)
+    assert e.value.name == "NTT_ERR_MISALIGNED"
+    p.close()
