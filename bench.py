@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--multiply-steps", type=int, default=10)
     ap.add_argument("--no-compressed", action="store_true")
     ap.add_argument("--no-small", action="store_true")
+    ap.add_argument("--no-u64", action="store_true")
     ap.add_argument("--compressed-steps", type=int, default=50)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=20000)
@@ -430,6 +431,8 @@ def run_ours(args):
         out["compressed_twiddles"] = bench_compressed(args, torch, nb, stream, d, P)
     if not args.no_small:
         out["small_sizes"] = bench_small(args, torch, nb, stream)
+    if not args.no_u64:
+        out["u64"] = bench_u64(args, torch, nb, stream)
     if not args.no_serve:
         out["serve"] = bench_serve(args, torch, nb)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -468,6 +471,9 @@ def summary(out):
         s["small_warp_speedup_vs_shared"] = {k: r(v["speedup_vs_shared"])
                                              for k, v in out["small_sizes"].items()
                                              if isinstance(v, dict)}
+    if "u64" in out:
+        s["u64_value"] = r(out["u64"]["value"], 1)
+        s["u64_hbm_frac"] = r(out["u64"]["roofline"]["frac"])
     if "compressed_twiddles" in out:
         ct = out["compressed_twiddles"]
         s["compressed_headline_ratio"] = r(ct["headline"]["speedup_vs_full"])
@@ -486,6 +492,47 @@ def summary(out):
 
 
 RAGGED = dict(seed=SEED, count=256, logn=tuple(range(12, 17)), limbs=(1, 48), bits=(30,))
+
+
+def bench_u64(args, torch, nb, stream):
+    """64-bit words: 16 polynomials of 2^16 x 16 limbs of primes below 2^60
+    (ntt64_find_moduli from 2^59; 128 MiB > L2), step = forward + inverse,
+    CUDA events.  Algorithmic bytes per launch: 16 per coefficient (read and
+    write of 8-byte words); the kernels run the column and the row stages as
+    two launches per direction, so their traffic is twice that."""
+    sh = stream.cuda_stream
+    logN, limbs, polys = 16, 16, 16
+    mods = nb.find_moduli64(logN, limbs, 1 << 59)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    x = torch.randint(0, 1 << 59, (polys * limbs << logN,), generator=g, device="cuda",
+                      dtype=torch.int64)
+    x0 = x.clone()
+    p = nb.Plan64(logN, mods)
+    with torch.cuda.stream(stream):
+        p.forward_many(x, polys, 0, sh)
+        p.inverse_many(x, polys, 0, sh)
+    stream.synchronize()
+    if not torch.equal(x, x0):
+        raise RuntimeError("64-bit roundtrip is not the identity")
+    del x0
+    K = 50
+    fwd = device_time(torch, stream, lambda: p.forward_many(x, polys, 0, sh), K, 3)
+    inv = device_time(torch, stream, lambda: p.inverse_many(x, polys, 0, sh), K, 3)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
+    alg = 16.0 * polys * limbs * (1 << logN)
+    dom = max(fwd, inv)
+    p.close()
+    return {"workload": f"{polys} x 2^{logN} x {limbs} limbs of primes below 2^60 (64-bit "
+                        "words), forward + inverse",
+            "value": 2 * polys * limbs / ((fwd + inv) / 1000.0), "unit": "limb-NTT/s",
+            "forward_ms": fwd, "inverse_ms": inv,
+            "roofline": {"bound": "hbm", "achieved": alg / (dom / 1000.0) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": alg / (dom / 1000.0) / 1e9 / peak,
+                         "algorithmic_bytes_per_launch": alg,
+                         "note": "two launches per direction: traffic is twice the "
+                                 "algorithmic bytes"}}
 
 
 def bench_small(args, torch, nb, stream):
