@@ -202,3 +202,33 @@ def test_plan64_validation_without_device():
     with pytest.raises(nb.NttError) as e:
         nb.Plan64(18, mods)
     assert e.value.name == "NTT_ERR_UNSUPPORTED"
+
+
+def test_new_entry_points_validate_before_device_work():
+    """Argument checks of the RNS steps, the spectrum product, compressed
+    plans and the small-kernel knob run before any CUDA call (no GPU
+    needed): NULL plans, unknown plan flags, compressed tables below logN 15."""
+    import ctypes
+    lib = nb._lib
+    null = ctypes.c_void_p(0)
+    calls = {
+        "ntt_forward_skip": lambda: lib.ntt_forward_skip(null, null, 1, 0, 0, 1, null),
+        "ntt_forward_sub_scale": lambda: lib.ntt_forward_sub_scale(null, null, 1, 0, null, 0, 0, 0,
+                                                                   null, null, null),
+        "ntt_inverse_scaled_range": lambda: lib.ntt_inverse_scaled_range(null, null, 1, 0, 0, 1,
+                                                                         null, null),
+        "ntt_multiply_spectrum_many": lambda: lib.ntt_multiply_spectrum_many(null, null, null, 1, 0,
+                                                                             null),
+        "ntt_plan_set_small_kernel": lambda: lib.ntt_plan_set_small_kernel(null, 0),
+    }
+    for name, call in calls.items():
+        assert nb.STATUS_NAMES[call()] == "NTT_ERR_INVALID_ARGUMENT", name
+    m = [(974258177, 3)]
+    arr, n = nb._moduli_array(m)
+    h = ctypes.c_void_p()
+    st = lib.ntt_plan_create_ex(16, arr, n, None, 0x80, ctypes.byref(h))
+    assert nb.STATUS_NAMES[st] == "NTT_ERR_INVALID_ARGUMENT"  # unknown flag
+    mods14 = O.ascending_primes(14, 1, 1 << 29)
+    with pytest.raises(nb.NttError) as e:
+        nb.Plan(14, mods14, compressed_twiddles=True)
+    assert e.value.name == "NTT_ERR_UNSUPPORTED"
