@@ -14,11 +14,12 @@
  *   layout:  limb-major, A[poly * poly_stride + limb * N + i], in place;
  *   psi = root^((q - 1) / 2N), table tw[i] = psi^bitrev(i, logN).
  * Arithmetic: 64-bit Shoup products with Harvey's lazy [0, 4q) ranges
- * (hence q < 2^62).  Kernels: logN <= 12 in one launch (a CTA per limb, all
- * stages in shared memory); larger sizes in two launches per direction (the
- * column stages, then the row stages, each CTA holding <= 2^12 words of a
- * few adjacent columns / rows in shared memory).  No reference counterpart
- * for the kernels themselves.
+ * (hence q < 2^62).  Kernels: logN <= 12 in one launch (a CTA per limb);
+ * larger sizes in two launches per direction (the column stages, then the
+ * row stages), each CTA holding <= 2^12 words of a few adjacent columns /
+ * rows in shared memory and running their stages as register passes of up
+ * to four stages (16 words per thread) with one barrier per pass.  No
+ * reference counterpart for the kernels themselves.
  */
 #ifndef NTT_B200_U64_H
 #define NTT_B200_U64_H

@@ -96,6 +96,100 @@ __device__ __forceinline__ uint32_t u64_off(const U64Args& a, uint32_t c, uint32
     return a.col ? c + (u << (a.n - a.k)) : (c << a.k) + u;
 }
 
+// Shared-memory index of local word u of sub-transform g (the layout the
+// coalesced loads and stores below use).
+__device__ __forceinline__ uint32_t u64_si(const U64Args& a, uint32_t g, uint32_t u) {
+    return a.col ? u * (uint32_t)a.G + g : (g << a.k) + u;
+}
+
+// One register pass over local bits [bmin, bmin + RP) of every sub-transform
+// the CTA holds: a thread takes 2^RP words whose local indices differ only in
+// those bits, runs the RP stages on them in registers (forward: from the
+// highest bit down; inverse: from the lowest up) and writes them back.
+template <int RP, bool Fwd>
+__device__ __forceinline__ void u64_pass(const U64Args& a, unsigned long long* s, uint32_t c0,
+                                         int bmin, const TwPair64* tw, uint64_t q) {
+    constexpr int W = 1 << RP;
+    const uint64_t q2 = 2 * q;
+    const uint32_t K = 1u << a.k, G = (uint32_t)a.G;
+    const uint32_t rest = K >> RP;  // local indices per group outside the pass's bits
+    const uint32_t groups = G * rest;
+    for (uint32_t grp = threadIdx.x; grp < groups; grp += blockDim.x) {
+        // consecutive threads: consecutive shared-memory words where possible
+        const uint32_t g = a.col ? grp % G : grp / rest;
+        const uint32_t ur = a.col ? grp / G : grp % rest;
+        const uint32_t ubase = ((ur >> bmin) << (bmin + RP)) | (ur & ((1u << bmin) - 1u));
+        uint64_t v[W];
+#pragma unroll
+        for (int j = 0; j < W; ++j) v[j] = s[u64_si(a, g, ubase | ((uint32_t)j << bmin))];
+#pragma unroll
+        for (int t = 0; t < RP; ++t) {
+            const int rb = Fwd ? RP - 1 - t : t;  // pass bit of this stage
+            const int b = bmin + rb;              // local bit
+            const int sg = a.col ? a.k - 1 - b : a.n - 1 - b;  // global stage
+            // the pair (j, j | 2^rb) sits at global distance 2^(n-1-sg), so its
+            // twiddle depends only on the pass bits above rb: block h of
+            // 2^rb pairs shares one, fetched with one 16-byte load just
+            // before its pairs (one live twiddle at a time)
+#pragma unroll
+            for (int h = 0; h < (W >> (rb + 1)); ++h) {
+                TwPair64 wh{0, 0};
+                if (sg != 0) {
+                    const uint32_t gi =
+                        u64_off(a, c0 + g, ubase | ((uint32_t)(h << (rb + 1)) << bmin));
+                    const ulonglong2 p = __ldg(
+                        reinterpret_cast<const ulonglong2*>(tw + (1u << sg) + (gi >> (a.n - sg))));
+                    wh = TwPair64{p.x, p.y};
+                }
+#pragma unroll
+                for (int lo = 0; lo < (1 << rb); ++lo) {
+                    const int j = (h << (rb + 1)) | lo;
+                    uint64_t X = v[j], Y = v[j | (1 << rb)];
+                    if (sg == 0) {
+                        const TwPair64 f = tw[0], fw = tw[1];
+                        if (Fwd) {
+                            const uint64_t A = shoup64(X, f, q), T = shoup64(Y, fw, q);
+                            X = A + T;
+                            Y = A - T + q2;
+                        } else {
+                            const uint64_t S = X + Y, D = X - Y + q2;
+                            X = csub64(shoup64(S, f, q), q);
+                            Y = csub64(shoup64(D, fw, q), q);
+                        }
+                    } else if (Fwd) {
+                        const uint64_t A = csub64(X, q2), T = shoup64(Y, wh, q);
+                        X = A + T;
+                        Y = A - T + q2;
+                    } else {
+                        const uint64_t S = X + Y, D = X - Y + q2;
+                        X = csub64(S, q2);
+                        Y = shoup64(D, wh, q);
+                    }
+                    v[j] = X;
+                    v[j | (1 << rb)] = Y;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < W; ++j) s[u64_si(a, g, ubase | ((uint32_t)j << bmin))] = v[j];
+    }
+}
+
+template <bool Fwd>
+__device__ __forceinline__ void u64_pass_rp(int rp, const U64Args& a, unsigned long long* s,
+                                            uint32_t c0, int bmin, const TwPair64* tw,
+                                            uint64_t q) {
+    switch (rp) {
+        case 1: u64_pass<1, Fwd>(a, s, c0, bmin, tw, q); break;
+        case 2: u64_pass<2, Fwd>(a, s, c0, bmin, tw, q); break;
+        case 3: u64_pass<3, Fwd>(a, s, c0, bmin, tw, q); break;
+        default: u64_pass<4, Fwd>(a, s, c0, bmin, tw, q); break;
+    }
+}
+
+// Stages [s0, s1) of the CTA's sub-transforms (every local bit of them: the
+// launches of run64 give each CTA whole column or row sub-transforms), in
+// register passes of up to four stages with one barrier between passes.
 template <bool Fwd>
 __global__ void __launch_bounds__(256) u64_stage_kernel(U64Args a) {
     extern __shared__ unsigned long long s[];
@@ -110,51 +204,26 @@ __global__ void __launch_bounds__(256) u64_stage_kernel(U64Args a) {
     const uint32_t c0 = group * G;
     // load: consecutive indices are consecutive words in global memory
     for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
-        uint32_t g, u, si;
-        if (a.col) { u = i / G; g = i - u * G; si = i; }
-        else { g = i >> a.k; u = i & (K - 1); si = i; }
-        s[si] = x[u64_off(a, c0 + g, u)];
+        uint32_t g, u;
+        if (a.col) { u = i / G; g = i - u * G; }
+        else { g = i >> a.k; u = i & (K - 1); }
+        s[i] = x[u64_off(a, c0 + g, u)];
     }
     __syncthreads();
-    const uint32_t half = total >> 1;
-    for (int st = 0; st < a.s1 - a.s0; ++st) {
-        const int sg = Fwd ? a.s0 + st : a.s1 - 1 - st;  // global stage
-        const int b = a.col ? a.k - 1 - sg : a.n - 1 - sg;  // local bit
-        for (uint32_t bf = threadIdx.x; bf < half; bf += blockDim.x) {
-            const uint32_t g = bf >> (a.k - 1), p = bf & ((K >> 1) - 1);
-            const uint32_t u = ((p >> b) << (b + 1)) | (p & ((1u << b) - 1));
-            const uint32_t v = u + (1u << b);
-            const uint32_t su = a.col ? u * G + g : (g << a.k) + u;
-            const uint32_t sv = a.col ? v * G + g : (g << a.k) + v;
-            uint64_t X = s[su], Y = s[sv];
-            const uint32_t gi = u64_off(a, c0 + g, u);
-            if (sg == 0) {
-                const TwPair64 f = tw[0], fw = tw[1];
-                if (Fwd) {
-                    const uint64_t A = shoup64(X, f, q), T = shoup64(Y, fw, q);
-                    X = A + T;
-                    Y = A - T + q2;
-                } else {
-                    const uint64_t S = X + Y, D = X - Y + q2;
-                    X = csub64(shoup64(S, f, q), q);
-                    Y = csub64(shoup64(D, fw, q), q);
-                }
-            } else {
-                const TwPair64 w = tw[(1u << sg) + (gi >> (a.n - sg))];
-                if (Fwd) {
-                    const uint64_t A = csub64(X, q2), T = shoup64(Y, w, q);
-                    X = A + T;
-                    Y = A - T + q2;
-                } else {
-                    const uint64_t S = X + Y, D = X - Y + q2;
-                    X = csub64(S, q2);
-                    Y = shoup64(D, w, q);
-                }
-            }
-            s[su] = X;
-            s[sv] = Y;
+    if (Fwd) {
+        for (int hi = a.k; hi > 0;) {
+            const int rp = hi < 4 ? hi : 4;
+            u64_pass_rp<true>(rp, a, s, c0, hi - rp, tw, q);
+            hi -= rp;
+            __syncthreads();
         }
-        __syncthreads();
+    } else {
+        for (int lo = 0; lo < a.k;) {
+            const int rp = a.k - lo < 4 ? a.k - lo : 4;
+            u64_pass_rp<false>(rp, a, s, c0, lo, tw, q);
+            lo += rp;
+            __syncthreads();
+        }
     }
     const bool canon = Fwd && a.s1 == a.n;  // the forward's last stage: canonical words
     for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
