@@ -175,7 +175,7 @@ __device__ __forceinline__ void u64_pass(const U64Args& a, unsigned long long* s
     }
 }
 
-template <bool Fwd>
+template <bool Fwd, int RPMAX>
 __device__ __forceinline__ void u64_pass_rp(int rp, const U64Args& a, unsigned long long* s,
                                             uint32_t c0, int bmin, const TwPair64* tw,
                                             uint64_t q) {
@@ -183,15 +183,25 @@ __device__ __forceinline__ void u64_pass_rp(int rp, const U64Args& a, unsigned l
         case 1: u64_pass<1, Fwd>(a, s, c0, bmin, tw, q); break;
         case 2: u64_pass<2, Fwd>(a, s, c0, bmin, tw, q); break;
         case 3: u64_pass<3, Fwd>(a, s, c0, bmin, tw, q); break;
-        default: u64_pass<4, Fwd>(a, s, c0, bmin, tw, q); break;
+        default:
+            if constexpr (RPMAX >= 4) u64_pass<4, Fwd>(a, s, c0, bmin, tw, q);
+            break;
     }
 }
 
+// Stages per register pass (8 words per thread at 3).  Measured on B200 at
+// 2^16 x 16 limbs x 16 polynomials, forward / inverse per launch pair:
+// four-stage passes 0.66 / 0.71 ms (124 registers, 2 CTAs per SM), three-stage
+// ones 0.50 / 0.45 ms, and 0.435 / 0.453 ms with the 4-CTA launch bound below
+// (64 registers).
+constexpr int kU64PassStages = 3;
+
 // Stages [s0, s1) of the CTA's sub-transforms (every local bit of them: the
 // launches of run64 give each CTA whole column or row sub-transforms), in
-// register passes of up to four stages with one barrier between passes.
+// register passes of up to kU64PassStages stages with one barrier between
+// passes.
 template <bool Fwd>
-__global__ void __launch_bounds__(256) u64_stage_kernel(U64Args a) {
+__global__ void __launch_bounds__(256, 4) u64_stage_kernel(U64Args a) {
     extern __shared__ unsigned long long s[];
     const uint32_t group = blockIdx.x % a.groups;
     const uint32_t lp = blockIdx.x / a.groups;  // limb-major: limb * polys + poly
@@ -210,17 +220,18 @@ __global__ void __launch_bounds__(256) u64_stage_kernel(U64Args a) {
         s[i] = x[u64_off(a, c0 + g, u)];
     }
     __syncthreads();
+    constexpr int R = kU64PassStages;
     if (Fwd) {
         for (int hi = a.k; hi > 0;) {
-            const int rp = hi < 4 ? hi : 4;
-            u64_pass_rp<true>(rp, a, s, c0, hi - rp, tw, q);
+            const int rp = hi < R ? hi : R;
+            u64_pass_rp<true, R>(rp, a, s, c0, hi - rp, tw, q);
             hi -= rp;
             __syncthreads();
         }
     } else {
         for (int lo = 0; lo < a.k;) {
-            const int rp = a.k - lo < 4 ? a.k - lo : 4;
-            u64_pass_rp<false>(rp, a, s, c0, lo, tw, q);
+            const int rp = a.k - lo < R ? a.k - lo : R;
+            u64_pass_rp<false, R>(rp, a, s, c0, lo, tw, q);
             lo += rp;
             __syncthreads();
         }
