@@ -63,9 +63,11 @@ namespace nttb {
 // schedule configuration for 16-limb batches larger than L2); otherwise the
 // first compiled configuration for logN.
 const FusedConfig* default_config(int logN, bool fwd) {
-    // split configurations first (measured on B200, 64 x 2^16 x 16 limbs:
-    // forward 0.234 / inverse 0.230 ms against 0.254 / 0.255 ms for the best
-    // cluster ones; ahead at 2^15 and 2^17 too)
+    // split configurations first, the first one of logN with 32-word passes
+    // in catalogue order (measured on B200, 64 x 2^16 x 16 limbs: forward
+    // 0.234 / inverse 0.230 ms against 0.254 / 0.255 ms for the best cluster
+    // ones; ahead at 2^15 and 2^17 too; at 2^15 the 8-CTA split takes 55.0 /
+    // 53.5 us per 32 x 16 limbs against 59.4 / 57.7 for the 4-CTA one)
     {
         const FusedConfig* c = fused_configs();
         for (int i = 0; i < fused_config_count(); ++i)
@@ -96,10 +98,19 @@ const FusedConfig* default_config(int logN, bool fwd) {
 // calls on B200, else the default for (logN, direction) when it carries one
 // polynomial per job, else the first such configuration.
 const FusedConfig* default_single_config(int logN, bool fwd) {
-    // split configurations first: one 2^16 x 16-limb polynomial per call took
-    // 13.2 / 12.3 us (forward / inverse) against 14.4 / 14.3 us for the best
-    // cluster configuration
-    if (const FusedConfig* d = default_config(logN, fwd); d && d->split) return d;
+    // split configurations first, the one with the most CTAs per limb (one
+    // wave of clusters: parallelism is latency).  Measured on B200, one
+    // 2^16 x 16-limb polynomial per call: 16-CTA split 12.3 / 10.3 us
+    // (forward / inverse), 8-CTA split 13.5 / 12.3 us, best cluster
+    // configuration 14.4 / 14.3 us.
+    {
+        const FusedConfig* c = fused_configs();
+        const FusedConfig* best = nullptr;
+        for (int i = 0; i < fused_config_count(); ++i)
+            if (c[i].split && c[i].logN == logN && c[i].eb == 5 && (!best || c[i].clog > best->clog))
+                best = &c[i];
+        if (best) return best;
+    }
     struct Pick {
         int logN, clog, r1, eb, k1a, k2a;
         bool fwd;

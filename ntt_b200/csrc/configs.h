@@ -39,8 +39,10 @@
 //   back to global memory; the limb's CTAs then exchange through L2 (in
 //   place) across one cluster barrier; phase 2 = passes of K2A, K2B and
 //   LOGN - EB - K2A - K2B (if nonzero) stages over the CTA's contiguous rows.
-#define NTTB_SPLIT_N16(S) S(16, 3, 5, 4, 4) S(16, 3, 4, 4, 4) S(16, 3, 5, 3, 4)
-#define NTTB_SPLIT_REST(S) S(17, 4, 5, 4, 4) S(15, 2, 5, 5, 5) S(15, 2, 4, 4, 4)
+#define NTTB_SPLIT_N16(S) \
+    S(16, 3, 5, 4, 4) S(16, 3, 4, 4, 4) S(16, 3, 5, 3, 4) S(16, 4, 5, 4, 4) S(16, 4, 4, 4, 4)
+#define NTTB_SPLIT_REST(S) \
+    S(17, 4, 5, 4, 4) S(15, 3, 5, 4, 3) S(15, 2, 5, 5, 5) S(15, 2, 4, 4, 4)
 #define NTTB_SPLIT_ALL(S) NTTB_SPLIT_N16(S) NTTB_SPLIT_REST(S)
 
 #include <cstdint>

@@ -236,6 +236,22 @@ struct SplitLayoutTable<16, 3, 5, 3, 4> {
 };
 
 template <>
+struct SplitLayoutTable<16, 4, 5, 4, 4> {
+    static constexpr int XW[5] = {5, 4, 8, 8, 4724};
+    static constexpr uint32_t lanes_P2A = 0x1fu;
+    static constexpr uint32_t lanes_P2B = 0x386u;
+    static constexpr uint32_t lanes_P2C = 0x3e0u;
+};
+
+template <>
+struct SplitLayoutTable<16, 4, 4, 4, 4> {
+    static constexpr int XW[5] = {5, 4, 8, 16, 4844};
+    static constexpr uint32_t lanes_P2A = 0x1fu;
+    static constexpr uint32_t lanes_P2B = 0x10fu;
+    static constexpr uint32_t lanes_P2C = 0x1f0u;
+};
+
+template <>
 struct SplitLayoutTable<17, 4, 5, 4, 4> {
     static constexpr int XW[5] = {5, 4, 8, 16, 9708};
     static constexpr uint32_t lanes_P2A = 0x1fu;
@@ -256,6 +272,14 @@ struct SplitLayoutTable<15, 2, 4, 4, 4> {
     static constexpr uint32_t lanes_P2A = 0x1fu;
     static constexpr uint32_t lanes_P2B = 0x187u;
     static constexpr uint32_t lanes_P2C = 0x1f0u;
+};
+
+template <>
+struct SplitLayoutTable<15, 3, 5, 4, 3> {
+    static constexpr int XW[5] = {5, 4, 12, 0, 4604};
+    static constexpr uint32_t lanes_P2A = 0x1fu;
+    static constexpr uint32_t lanes_P2B = 0x3c4u;
+    static constexpr uint32_t lanes_P2C = 0x3e0u;
 };
 
 }  // namespace nttb
