@@ -65,6 +65,9 @@ const std::vector<Entry>& entries() {
 std::string g_err;
 }  // namespace
 
+extern const SplitEntry kEmuSplit[];
+extern const int kEmuSplitCount;
+
 }  // namespace emu
 
 using namespace emu;
@@ -93,5 +96,20 @@ int emu_transform(int i, int mode, uint32_t* data, const uint32_t* tw_pairs, con
     return fn(mode & 1, data, tw_pairs, q, limbs, stats, g_err);
 }
 const char* emu_last_error() { return g_err.c_str(); }
+// Split configurations (NTTB_SPLIT_ALL order).  out7: N, CL, EB, K2A, K2B,
+// threads, shared-memory bytes.
+int emu_num_split() { return kEmuSplitCount; }
+void emu_split_config(int i, int* out7) {
+    for (int k = 0; k < 5; ++k) out7[k] = kEmuSplit[i].v[k];
+    out7[5] = kEmuSplit[i].threads;
+    out7[6] = (int)kEmuSplit[i].smem;
+}
+// mode bit 0: forward (else inverse); bit 2: compressed tables.
+int emu_split_transform(int i, int mode, uint32_t* data, const uint32_t* tw_pairs,
+                        const uint32_t* q, int limbs, double* stats) {
+    g_err.clear();
+    RunFn fn = (mode & 4) ? kEmuSplit[i].comp : kEmuSplit[i].full;
+    return fn(mode & 1, data, tw_pairs, q, limbs, stats, g_err);
+}
 void emu_set_dump(uint32_t* p) { g_dump = p; }
 }

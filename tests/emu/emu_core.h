@@ -23,6 +23,7 @@
 
 #include "../../ntt_b200/csrc/configs.h"
 #include "../../ntt_b200/csrc/ntt_core.cuh"
+#include "../../ntt_b200/csrc/split_geo.cuh"
 
 using namespace nttb;
 
@@ -452,4 +453,136 @@ constexpr RunFn comp_run() {
      &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A, NP), (NP) == 1>,                              \
      &run_cfg<EMU_G(N, CL, R1, EB, K1A, K2A, NP), false>,                                  \
      comp_run<EMU_G(N, CL, R1, EB, K1A, K2A, NP)>()},
+// ---------------------------------------------------------------------------
+// Split configurations (split_geo.cuh): phase 1 straight from and back to
+// global memory, the cluster barrier (here: the end of a step over every CTA),
+// then the phase-2 passes in the work buffer and the chunked store.  The same
+// checks as the cluster kernels: bounds, every work-buffer word of a pass and
+// every global word of each phase written exactly once, warp-local reads
+// after warp barriers, bank conflicts; bit-exact results against the oracle.
+// ---------------------------------------------------------------------------
+template <class G, class Arith, bool Fwd, bool Comp>
+int run_split_limb(uint32_t* limb, const TwPair* tw, uint32_t q, Stats& st, std::string& err) {
+    using Ctx = EmuCtx<false, Comp>;
+    constexpr uint32_t N = 1u << G::LOGN;
+    constexpr uint32_t kTwLen = Comp ? tw_comp_entries(G::LOGN) : N;
+    EmuCluster cl;
+    cl.C = G::C;
+    cl.smem_words = G::SLAB_WORDS;
+    cl.smem.assign(G::C, std::vector<uint32_t>(G::SLAB_WORDS, 0xDEADBEEFu));
+    cl.writes.assign(G::C, std::vector<uint32_t>(G::SLAB_WORDS, 0));
+    cl.shadow.assign(G::C, std::vector<uint32_t>(G::SLAB_WORDS, 0));
+    cl.rwrites.assign(G::C, std::vector<uint32_t>(G::SLAB_WORDS, 0));
+    cl.writer.assign(G::C, std::vector<uint32_t>(G::SLAB_WORDS, 0xFFFFFFFFu));
+    std::vector<uint32_t> words(limb, limb + N);
+    uint32_t* gp[1] = {words.data()};
+    std::vector<uint32_t> gw[1] = {std::vector<uint32_t>(N, 0)};
+    auto mk = [&](uint32_t rank) {
+        Ctx c{&cl, gp, N, tw, kTwLen, q, 2 * q, rank};
+        c.gwrites = gw;
+        return c;
+    };
+    auto step = [&](auto fn, bool warp_local) {
+        cl.warp_local = warp_local;
+        for (auto& w : cl.writes) std::fill(w.begin(), w.end(), 0u);
+        for (uint32_t r = 0; r < (uint32_t)G::C; ++r) {
+            Ctx c = mk(r);
+            for (uint32_t t = 0; t < (uint32_t)G::THREADS; ++t) {
+                c.tid = t;
+                c.seq = 0;
+                fn(c, t);
+            }
+        }
+        account(cl, st);
+    };
+    auto check_cover = [&](const char* what) {
+        for (int r = 0; r < G::C; ++r)
+            for (uint32_t lam = 0; lam < G::M; ++lam)
+                if (cl.writes[r][G::XW::phys(lam)] != 1) {
+                    if (err.empty()) err = std::string(what) + ": word not written exactly once";
+                    return;
+                }
+    };
+    auto check_global = [&](const char* what) {
+        for (uint32_t i = 0; i < N; ++i)
+            if (gw[0][i] != 1) {
+                if (err.empty()) err = std::string(what) + ": global word not written exactly once";
+                return;
+            }
+        std::fill(gw[0].begin(), gw[0].end(), 0u);
+    };
+    if constexpr (Fwd) {
+        using F = SplitFwd<G, Arith, Ctx>;
+        step([](Ctx& c, uint32_t t) { F::p1(c, t); }, false);
+        check_global("phase 1");
+        step([](Ctx& c, uint32_t t) { F::p2a(c, t); }, false);
+        check_cover("pass 2a");
+        step([](Ctx& c, uint32_t t) { F::p2b(c, t); }, G::kABWarp);
+        check_cover("pass 2b");
+        if constexpr (G::K2C > 0) {
+            step([](Ctx& c, uint32_t t) { F::p2c(c, t); }, G::kBCWarp);
+            check_cover("pass 2c");
+        }
+        step([](Ctx& c, uint32_t t) { F::out(c, t); }, G::kChunkWarp);
+        check_global("output");
+    } else {
+        using I = SplitInv<G, Arith, Ctx>;
+        step([](Ctx& c, uint32_t t) { I::in(c, t); }, false);
+        check_cover("slab in");
+        if constexpr (G::K2C > 0) {
+            step([](Ctx& c, uint32_t t) { I::p2c(c, t); }, G::kChunkWarp);
+            check_cover("pass 2c");
+            step([](Ctx& c, uint32_t t) { I::p2b(c, t); }, G::kBCWarp);
+        } else {
+            step([](Ctx& c, uint32_t t) { I::p2b(c, t); }, G::kChunkWarp);
+        }
+        check_cover("pass 2b");
+        step([](Ctx& c, uint32_t t) { I::p2a(c, t); }, G::kABWarp);
+        check_global("phase 2");
+        step([](Ctx& c, uint32_t t) { I::p1(c, t); }, false);
+        check_global("phase 1");
+    }
+    if (!cl.err.empty() && err.empty()) err = cl.err;
+    if (!err.empty()) return 1;
+    std::copy(words.begin(), words.end(), limb);
+    return 0;
+}
+
+template <class G, bool Comp>
+int run_split_cfg(int fwd, uint32_t* data, const uint32_t* tw_pairs, const uint32_t* q, int limbs,
+                  double* stats, std::string& err) {
+    Stats st;
+    const size_t N = size_t{1} << G::LOGN;
+    const size_t TWS = Comp ? tw_comp_entries(G::LOGN) : N;
+    for (int l = 0; l < limbs; ++l) {
+        const TwPair* tw = reinterpret_cast<const TwPair*>(tw_pairs) + l * TWS;
+        int rc;
+        if (q[l] < (1u << 30))
+            rc = fwd ? run_split_limb<G, Lazy4, true, Comp>(data + l * N, tw, q[l], st, err)
+                     : run_split_limb<G, Lazy4, false, Comp>(data + l * N, tw, q[l], st, err);
+        else
+            rc = fwd ? run_split_limb<G, Lazy2, true, Comp>(data + l * N, tw, q[l], st, err)
+                     : run_split_limb<G, Lazy2, false, Comp>(data + l * N, tw, q[l], st, err);
+        if (rc) return rc;
+    }
+    if (stats) {
+        stats[0] = st.worst;
+        stats[1] = st.n ? st.sum / st.n : 0;
+    }
+    return 0;
+}
+
+struct SplitEntry {
+    int v[5];
+    int threads;
+    unsigned smem;
+    RunFn full, comp;  // full / compressed twiddle tables
+};
+
+#define EMU_SG(N, CL, EB, KA, KB) SplitGeo<N, CL, EB, KA, KB>
+#define EMU_SPLIT_ENTRY(N, CL, EB, KA, KB)                                                       \
+    {{N, CL, EB, KA, KB}, EMU_SG(N, CL, EB, KA, KB)::THREADS, EMU_SG(N, CL, EB, KA, KB)::SMEM_BYTES, \
+     &run_split_cfg<EMU_SG(N, CL, EB, KA, KB), false>,                                            \
+     &run_split_cfg<EMU_SG(N, CL, EB, KA, KB), true>},
+
 }  // namespace emu

@@ -1,4 +1,5 @@
-"""Index maps of every compiled fused-kernel configuration, checked on the CPU.
+"""Index maps of every compiled fused-kernel and split-kernel configuration,
+checked on the CPU.
 
 tests/emu/libntt_emu.so runs the device kernels' pass functions
 (ntt_b200/csrc/ntt_core.cuh) thread by thread on the host.  Each
@@ -111,3 +112,55 @@ def test_compressed_tables_factor_the_full_ones():
                 base = tab[h + (j // f) * f].astype(np.uint64)
                 lsb = tab[(j % f)].astype(np.uint64)
                 assert np.array_equal((base * lsb) % np.uint64(q), tab[h + j].astype(np.uint64))
+
+
+def split_configs():
+    # the split list in NTTB_SPLIT_ALL order (NTTB_SPLIT_N16, then NTTB_SPLIT_REST)
+    import re
+    src = open(os.path.join(os.path.dirname(__file__), "..", "ntt_b200", "csrc", "configs.h")).read()
+    out = []
+    for name in ("NTTB_SPLIT_N16", "NTTB_SPLIT_REST"):
+        body = src.split(f"#define {name}(S)")[1].split("#define")[0]
+        out += [tuple(int(v) for v in m)
+                for m in re.findall(r"S\((\d+), (\d+), (\d+), (\d+), (\d+)\)", body)]
+    return out
+
+
+@pytest.mark.parametrize("idx,cfg", list(enumerate(split_configs())), ids=lambda v: str(v))
+@pytest.mark.parametrize("bits", [30, 31])
+@pytest.mark.parametrize("compressed", [False, True], ids=["full", "compressed"])
+def test_split_config_matches_oracle(emu, idx, cfg, bits, compressed):
+    """The split kernels' passes (split_geo.cuh) run thread by thread: phase 1
+    in place in global memory, the cluster barrier between steps, the phase-2
+    passes in the work buffer.  Bit-exact against the oracle, every access in
+    bounds, every word of each pass and phase written exactly once, warp-local
+    reads after warp barriers, bank conflicts at most 4-way; full and
+    compressed twiddle tables."""
+    emu.emu_split_config.argtypes = [ctypes.c_int, ctypes.c_void_p]
+    emu.emu_split_transform.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.c_void_p]
+    assert emu.emu_num_split() == len(split_configs())
+    c = (ctypes.c_int * 7)()
+    emu.emu_split_config(idx, c)
+    assert tuple(c)[:5] == cfg
+    logN = cfg[0]
+    start = int(2 ** 29.5) if bits == 30 else int(2 ** 30.5)
+    mods = O.ascending_primes(logN, 2, start)
+    T = O.LimbTables(logN, mods)
+    fwd, inv = compressed_tables(T) if compressed else device_tables(T)
+    x = O.uniform_limbs(logN, T.q, 500 + idx)
+    x[0, :3] = [0, T.q[0] - 1, 0xFFFFFFFF]
+    d = x.copy()
+    st = (ctypes.c_double * 2)()
+    mode = 4 if compressed else 0
+    rc = emu.emu_split_transform(idx, 1 | mode, d.ctypes.data, fwd.ctypes.data, T.q.ctypes.data, 2, st)
+    assert rc == 0, emu.emu_last_error().decode()
+    assert np.array_equal(d, T.forward_mont(x))
+    assert st[0] <= 4
+    rc = emu.emu_split_transform(idx, mode, d.ctypes.data, inv.ctypes.data, T.q.ctypes.data, 2, st)
+    assert rc == 0, emu.emu_last_error().decode()
+    expect = x.copy()
+    expect[0, 2] = 0xFFFFFFFF % T.q[0]
+    assert np.array_equal(d, expect)
+    assert st[0] <= 4
