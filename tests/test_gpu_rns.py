@@ -187,3 +187,46 @@ def test_rns_errors(torch_cuda):
         # an empty subtrahend range is the scaled forward
         plan.forward_sub_scale(a, None, 2, 2)
         torch.cuda.synchronize()
+
+
+def test_rns_steps_at_full_size(torch_cuda):
+    """2^17 x 64 limbs (the largest plan), no oracle: ModUp's forward equals
+    the plain forward on every limb outside the skipped range and leaves that
+    range alone; ModDown's forward against the plain forward's own spectrum is
+    zero; the scaled inverse of a limb range undoes the forward there; the
+    product with a resident spectrum equals the unfused calls."""
+    torch = torch_cuda
+    import ntt_b200 as nb
+    logN, limbs = 17, 64
+    mods = plan_moduli(logN, limbs, 31)
+    q = np.array([m[0] for m in mods], dtype=np.uint64)
+    N = 1 << logN
+    x = O.uniform_limbs(logN, q, 2024)
+    with nb.Plan(logN, mods) as plan:
+        plain = to_dev(torch, x)
+        plan.forward(plain)
+        skip = to_dev(torch, x)
+        plan.forward_skip(skip, 20, 44)
+        sub = to_dev(torch, x)
+        plan.forward_sub_scale(sub, plain.clone(), 0, limbs, None, None)
+        torch.cuda.synchronize()
+        P, S = to_host(plain, x.shape), to_host(skip, x.shape)
+        assert np.array_equal(S[:20], P[:20]) and np.array_equal(S[44:], P[44:])
+        assert np.array_equal(S[20:44], x[20:44])
+        assert not to_host(sub, x.shape).any()
+        back = plain.clone()
+        plan.inverse_scaled_range(back, 8, 40, None)
+        torch.cuda.synchronize()
+        B = to_host(back, x.shape)
+        assert np.array_equal(B[8:40], x[8:40])
+        assert np.array_equal(B[:8], P[:8]) and np.array_equal(B[40:], P[40:])
+        # product with a resident spectrum vs forward, pointwise, inverse
+        y = O.uniform_limbs(logN, q, 2025)
+        b1, b2 = to_dev(torch, y), to_dev(torch, y)
+        plan.multiply_spectrum_many(plain, b1, 1)
+        plan.forward(b2)
+        plan.pointwise_mul(b2, plain, b2)
+        plan.inverse(b2)
+        torch.cuda.synchronize()
+        assert torch.equal(b1, b2)
+        assert N * limbs == b1.numel()
