@@ -7,7 +7,11 @@
 // picked per (logN, limb count, direction) at run time, "sweep, then cache".
 // Cache file: $NTT_B200_TUNE_CACHE, else $HOME/.cache/ntt_b200/tune.txt;
 // one line per entry:
-//   "<device-name>|<sm-count> <logN> <limb-bucket> <fwd|inv> <config-index> <us>".
+//   "<device-name>|<sm-count> <logN> <limb-bucket> <fwd|inv> <config> <us>",
+// <config> the configuration's parameters (config_signature), not its
+// catalogue index, so that a cache written by another build of the library
+// never selects a different kernel: entries whose configuration is not
+// compiled here are ignored.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -56,17 +60,31 @@ std::string cache_path() {
     return std::string(h ? h : "/tmp") + "/.cache/ntt_b200/tune.txt";
 }
 
+// "logN,CTAs,r1,eb,k1a,k2a,polys-per-job,exchange,k2b" (ntt_kernel_config_t's fields).
+std::string config_signature(const FusedConfig* c) {
+    char b[96];
+    snprintf(b, sizeof b, "%d,%d,%d,%d,%d,%d,%d,%d,%d", c->logN, 1 << c->clog, c->r1, c->eb, c->k1a,
+             c->k2a, c->np, c->split, c->split ? c->k2b : 0);
+    return b;
+}
+
+int config_by_signature(const std::string& sig) {
+    for (int i = 0; i < fused_config_count(); ++i)
+        if (config_signature(config_by_index(i)) == sig) return i;
+    return -1;
+}
+
 void load_locked() {
     if (g_loaded) return;
     g_loaded = true;
     FILE* f = fopen(cache_path().c_str(), "r");
     if (!f) return;
-    char dev[256], dir[8];
-    int logN, bucket, idx;
+    char dev[256], dir[8], sig[96];
+    int logN, bucket;
     double us;
-    while (fscanf(f, "%255s %d %d %7s %d %lf", dev, &logN, &bucket, dir, &idx, &us) == 6) {
-        const FusedConfig* c = config_by_index(idx);
-        if (c && c->logN == logN)
+    while (fscanf(f, "%255s %d %d %7s %95s %lf", dev, &logN, &bucket, dir, sig, &us) == 6) {
+        const int idx = config_by_signature(sig);
+        if (idx >= 0 && config_by_index(idx)->logN == logN)
             g_table[{dev, logN, bucket, std::string(dir) == "fwd" ? 1 : 0}] = {idx, us};
     }
     fclose(f);
@@ -80,9 +98,9 @@ void save_locked() {
     FILE* f = fopen(path.c_str(), "w");
     if (!f) return;
     for (auto& kv : g_table)
-        fprintf(f, "%s %d %d %s %d %.3f\n", std::get<0>(kv.first).c_str(), std::get<1>(kv.first),
-                std::get<2>(kv.first), std::get<3>(kv.first) ? "fwd" : "inv", kv.second.first,
-                kv.second.second);
+        fprintf(f, "%s %d %d %s %s %.3f\n", std::get<0>(kv.first).c_str(), std::get<1>(kv.first),
+                std::get<2>(kv.first), std::get<3>(kv.first) ? "fwd" : "inv",
+                config_signature(config_by_index(kv.second.first)).c_str(), kv.second.second);
     fclose(f);
 }
 

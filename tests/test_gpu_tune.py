@@ -49,9 +49,16 @@ def test_sweep_writes_cache_and_a_fresh_process_reuses_it(tune_cache):
     assert r.candidates == len(cands)
     assert r.fwd_index in cands and r.inv_index in cands
     assert r.fwd_us > 0 and r.inv_us > 0
+    # entries name configurations by their parameters, not catalogue indices
+    cfgs = nb.kernel_configs()
+
+    def sig(i):
+        c = cfgs[i]
+        return ",".join(str(v) for v in (c.logN, c.cluster_ctas, c.r1, c.words_log2, c.k1a, c.k2a,
+                                         c.polys_per_job, c.exchange, c.k2b if c.exchange else 0))
     lines = [l.split() for l in path.read_text().splitlines()]
-    mine = {l[3]: int(l[4]) for l in lines if int(l[1]) == logN}
-    assert mine == {"fwd": r.fwd_index, "inv": r.inv_index}
+    mine = {l[3]: l[4] for l in lines if int(l[1]) == logN}
+    assert mine == {"fwd": sig(r.fwd_index), "inv": sig(r.inv_index)}
     # a plan in this process and one in a fresh process both take the entry
     mods = [(m.qi, m.primitive_root) for m in nb.find_moduli(logN, limbs, 1 << 29)]
     with nb.Plan(logN, mods) as p:
@@ -84,3 +91,19 @@ def test_tuned_plans_are_bit_exact(tune_cache, logN, limbs):
         p.inverse(d)
         torch.cuda.synchronize()
         assert np.array_equal(d.cpu().numpy().view(np.uint32), x)
+
+
+def test_cache_entries_of_unknown_configurations_are_ignored(tune_cache):
+    """A cache written by another build may name configurations this build
+    does not compile (or bare catalogue indices of an older format): such
+    entries are skipped, and plans stay on the defaults."""
+    nb, path = tune_cache
+    r = nb.autotune(14, 2, polys=2, iters=1)  # writes the file: learn this device's key
+    dev = path.read_text().split()[0]
+    path.write_text(f"{dev} 16 1 fwd 16,8,9,5,3,4,1,0,0 1.0\n"   # not compiled
+                    f"{dev} 16 1 inv 26 1.0\n")                  # old index format
+    nb.autotune_reload()
+    mods = [(m.qi, m.primitive_root) for m in nb.find_moduli(16, 3, 1 << 29)]
+    with nb.Plan(16, mods) as p:
+        assert p.info.tuned == 0
+    assert r.candidates > 0
