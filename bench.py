@@ -467,6 +467,7 @@ def summary(out):
         s["multiply_speedup_vs_unfused"] = r(fm["speedup_vs_unfused"])
         s["multiply_batch_tiles_speedup_vs_unfused"] = r(fm["batch_tiles"]["speedup_vs_unfused"])
         s["multiply_spectrum_speedup_vs_unfused"] = r(fm["spectrum"]["speedup_vs_unfused"])
+        s["multiply_one_launch_speedup_vs_unfused"] = r(fm["one_launch"]["speedup_vs_unfused"])
     if "small_sizes" in out:
         s["small_warp_speedup_vs_shared"] = {k: r(v["speedup_vs_shared"])
                                              for k, v in out["small_sizes"].items()
@@ -752,10 +753,13 @@ def kernel_name(nb, info, direction):
 def bench_multiply(args, torch, nb, stream):
     """Fused negacyclic multiply: 128 pairs of 2^16 x 24-limb polynomials
     (24 ascending 30-bit primes q == 1 mod 2^17 above 2^29.5), uniform [0, q)
-    coefficients; c = a * b into b's buffer.  Fused: ntt_multiply_many, one
-    launch with a thread-block cluster per (pair, limb) job: NTT(b), NTT(a),
-    the pointwise Montgomery product and INTT per limb, a read once and b
-    read and written once (12 bytes per coefficient).  Unfused: the plain calls
+    coefficients; c = a * b into b's buffer.  Fused: ntt_multiply_many in its
+    default form on this split plan -- NTT(b) with the split kernel, NTT(a)
+    with the pointwise Montgomery product folded into its store into b (a
+    cluster kernel: a is only read), INTT(b) with the split kernel (28 bytes
+    per coefficient) -- and, as `one_launch`, the split multiply kernel (NTT(b),
+    NTT(a), product and INTT per (pair, limb) in one launch: a read once, b
+    read and written once, 12 bytes per coefficient).  Unfused: the plain calls
     forward_many(a), forward_many(b), pointwise_mul, inverse_many(b) (4
     launches, 36 bytes per coefficient; a is overwritten by its spectrum,
     which favours it).  Batch tiles: the same products as multiply tiles of
@@ -784,6 +788,7 @@ def bench_multiply(args, torch, nb, stream):
     if not torch.equal(b, tb):
         raise RuntimeError("batch-tile and unfused multiply differ")
     pb = b0.clone()
+    b3 = b0.clone()  # the three-launch form's operand (b holds the tiles' product by now)
     with torch.cuda.stream(stream):
         p.multiply_many(a, pb, pairs, 0, sh)
     stream.synchronize()
@@ -824,6 +829,19 @@ def bench_multiply(args, torch, nb, stream):
     del su
     fused_ms = device_time(torch, stream, lambda: p.multiply_many(a, pb, pairs, 0, sh),
                            args.multiply_steps, w)
+    # the one-launch form on the same (split) plan
+    p3 = nb.Plan(logN, mods)
+    p3.set_multiply_form(nb.MULTIPLY_ONE_LAUNCH)
+    p3b = b3
+    with torch.cuda.stream(stream):
+        p3.multiply_many(a, p3b, pairs, 0, sh)
+    stream.synchronize()
+    if not torch.equal(p3b, tb):
+        raise RuntimeError("one-launch and unfused multiply differ")
+    one_ms = device_time(torch, stream, lambda: p3.multiply_many(a, p3b, pairs, 0, sh),
+                           args.multiply_steps, w)
+    p3.close()
+    del p3b
     unfused_ms = device_time(torch, stream, unfused, args.multiply_steps, w)
     tiles_ms = device_time(torch, stream, lambda: tiles.run(sh), args.multiply_steps, w)
     products = pairs * limbs
@@ -833,14 +851,18 @@ def bench_multiply(args, torch, nb, stream):
                     "c = a*b negacyclic per limb into b",
         "value": products / (fused_ms / 1000.0), "unit": "limb-products/s",
         "limb_ntt_per_s": 3 * products / (fused_ms / 1000.0),
-        "ms_per_step": fused_ms, "launches_per_step": 1,
-        "form": "ntt_multiply_many: one launch, a cluster per (pair, limb): NTT(b), NTT(a), "
-                "product, INTT",
-        "algorithmic_bytes": 12 * words,
-        "achieved_gbs": 12 * words / (fused_ms / 1000.0) / 1e9,
+        "ms_per_step": fused_ms, "launches_per_step": 3,
+        "form": "ntt_multiply_many (default form on split plans: split NTT(b), cluster NTT(a) "
+                "with the product folded into its store into b, split INTT(b))",
+        "algorithmic_bytes": 28 * words,
+        "achieved_gbs": 28 * words / (fused_ms / 1000.0) / 1e9,
         "unfused": {"value": products / (unfused_ms / 1000.0), "ms_per_step": unfused_ms,
                     "launches_per_step": 4, "algorithmic_bytes": 36 * words},
         "speedup_vs_unfused": unfused_ms / fused_ms,
+        "one_launch": {"form": "the split multiply kernel: NTT(b), NTT(a), product, INTT per "
+                               "(pair, limb) in one launch",
+                       "value": products / (one_ms / 1000.0), "ms_per_step": one_ms,
+                       "launches_per_step": 1, "speedup_vs_unfused": unfused_ms / one_ms},
         "spectrum": {"form": "ntt_multiply_spectrum_many with NTT(a) resident: forward of b "
                              "with the product on its final store, inverse (2 launches)",
                      "value": products / (spec_ms / 1000.0), "ms_per_step": spec_ms,

@@ -249,14 +249,15 @@ NTT_API ntt_status_t ntt_pointwise_mul(const ntt_plan_t* plan, uint32_t* c_dev,
                                        size_t poly_stride, ntt_stream_t stream);
 /* b <- a * b, the negacyclic product per limb modulus (normal domain in and
  * out, canonical words), for `polys` pairs (poly_stride words apart, 0 =
- * packed; 16-byte aligned; a is read only and must not overlap b).  Plans
- * whose forward configuration is a split one (the default for logN 15..17)
- * run it in ONE launch: per limb NTT(b), NTT(a), the Montgomery product and
- * INTT, with b's buffer carrying the intermediate words through L2 (HBM
- * reads a and b once and writes b once).  Other plans use three launches of
- * their transform kernels: NTT(b) in place; NTT(a) with the pointwise product
- * folded into its store; INTT(b).  Either way the same result as
- * ntt_forward_many on both, ntt_pointwise_mul, then ntt_inverse_many.
+ * packed; 16-byte aligned; a is read only and must not overlap b).  Three
+ * launches: NTT(b) in place; NTT(a) with the pointwise Montgomery product
+ * folded into its store into b (a cluster configuration, whose phases meet in
+ * shared memory, so a is only read); INTT(b).  Plans whose forward is a split
+ * configuration (logN 15..17) run the first and last with the split kernels,
+ * and can run the whole product in one launch of the split multiply kernel
+ * instead (ntt_plan_set_multiply_form, include/ntt_b200_tune.h; slower on
+ * B200: 3 CTAs per SM for its two work buffers).  Either way the same result
+ * as ntt_forward_many on both, ntt_pointwise_mul, then ntt_inverse_many.
  * logN >= 10.  No reference counterpart (the reference has no product). */
 NTT_API ntt_status_t ntt_multiply_many(const ntt_plan_t* plan, const uint32_t* a_dev,
                                        uint32_t* b_dev, size_t polys, size_t poly_stride,

@@ -71,6 +71,18 @@ NTT_API ntt_status_t ntt_plan_set_schedule(ntt_plan_t* plan, int schedule);
 #define NTT_SMALL_WARP 0
 #define NTT_SMALL_SHARED 1
 NTT_API ntt_status_t ntt_plan_set_small_kernel(ntt_plan_t* plan, int kind);
+/* Form of ntt_multiply_many on plans whose forward is a split configuration
+ * (results identical):
+ * NTT_MULTIPLY_ONE_LAUNCH: NTT(b), NTT(a), product and INTT per (pair, limb)
+ *   in one launch of the split multiply kernel;
+ * NTT_MULTIPLY_THREE_LAUNCHES: NTT(b) (split kernel), NTT(a) with the product
+ *   folded into its store into b (a cluster kernel: a is only read), INTT(b)
+ *   (split kernel); the default, measured faster on B200 (2.09 against
+ *   2.37 ms for 128 pairs of 2^16 x 24 limbs).  Other plans always run the
+ *   three-launch form. */
+#define NTT_MULTIPLY_ONE_LAUNCH 0
+#define NTT_MULTIPLY_THREE_LAUNCHES 1
+NTT_API ntt_status_t ntt_plan_set_multiply_form(ntt_plan_t* plan, int form);
 /* Self-test of the kernels' failure detection (no reference counterpart):
  * runs, on `stream`, the bounded mbarrier wait the transform kernels use,
  * on a barrier that nothing ever completes, with a limit of `limit` tries

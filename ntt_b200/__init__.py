@@ -101,6 +101,7 @@ class TuneResult(ctypes.Structure):
 NTT_OK = 0
 PLAN_COMPRESSED_TWIDDLES = 1  # include/ntt_b200.h: NTT_PLAN_COMPRESSED_TWIDDLES
 SMALL_WARP, SMALL_SHARED = 0, 1  # include/ntt_b200_tune.h: NTT_SMALL_*
+MULTIPLY_ONE_LAUNCH, MULTIPLY_THREE_LAUNCHES = 0, 1  # NTT_MULTIPLY_*
 STATUS_NAMES = {
     0: "NTT_OK", 1: "NTT_ERR_INVALID_ARGUMENT", 2: "NTT_ERR_MODULUS", 3: "NTT_ERR_ROOT",
     4: "NTT_ERR_MODULUS_RANGE", 5: "NTT_ERR_UNSUPPORTED", 6: "NTT_ERR_MISALIGNED",
@@ -170,6 +171,7 @@ _sig("ntt_autotune_forget", None)
 _sig("ntt_plan_force_config", _st, _vp, ctypes.c_int, ctypes.c_int)
 _sig("ntt_plan_set_schedule", _st, _vp, ctypes.c_int)
 _sig("ntt_plan_set_small_kernel", _st, _vp, ctypes.c_int)
+_sig("ntt_plan_set_multiply_form", _st, _vp, ctypes.c_int)
 _sig("ntt_plan_check", _st, _vp, ctypes.POINTER(ctypes.c_uint32))
 _sig("ntt_config_resident_clusters", ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
 SCHEDULE_DIRECT = 0
@@ -324,6 +326,12 @@ class Plan:
     def force_config(self, fwd_index: int = -1, inv_index: int = -1):
         """Pin the plan to compiled configurations (see kernel_configs())."""
         _check(_lib.ntt_plan_force_config(self._h, fwd_index, inv_index), "ntt_plan_force_config")
+
+    def set_multiply_form(self, form: int = MULTIPLY_ONE_LAUNCH):
+        """Split plans: multiply_many in one launch (MULTIPLY_ONE_LAUNCH) or
+        as split forward, cluster forward with the product, split inverse
+        (MULTIPLY_THREE_LAUNCHES)."""
+        _check(_lib.ntt_plan_set_multiply_form(self._h, form), "ntt_plan_set_multiply_form")
 
     def set_small_kernel(self, kind: int = SMALL_WARP):
         """logN 6..9: SMALL_WARP (a warp per limb, shuffles) or SMALL_SHARED

@@ -332,6 +332,11 @@ struct ntt_plan {
     bool lazy2 = false;  // a modulus >= 2^30: every limb uses the [0, 2q) discipline
     bool compressed = false;  // compressed twiddle tables (split configurations only)
     bool small_shared = false;  // logN 6..9: the shared-memory kernel instead of the warp one
+    // split plans: ntt_multiply_many's form.  Measured on B200 (128 pairs x
+    // 2^16 x 24 limbs): three launches 2.09 ms, one launch 2.37 ms, the unfused
+    // calls 2.28 ms (the one-launch kernel's second work buffer caps it at 3
+    // CTAs per SM against 5 for the split transforms)
+    int multiply_form = NTT_MULTIPLY_THREE_LAUNCHES;
     size_t tw_stride = 0;     // table pairs per limb: N, or tw_comp_entries(logN)
 };
 
@@ -670,6 +675,14 @@ ntt_status_t ntt_selftest_wait_expiry(const ntt_plan_t* p, uint32_t limit, ntt_s
     return NTT_OK;
 }
 
+ntt_status_t ntt_plan_set_multiply_form(ntt_plan_t* p, int form) {
+    if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
+    if (form != NTT_MULTIPLY_ONE_LAUNCH && form != NTT_MULTIPLY_THREE_LAUNCHES)
+        return fail(NTT_ERR_INVALID_ARGUMENT, "unknown multiply form %d", form);
+    p->multiply_form = form;
+    return NTT_OK;
+}
+
 ntt_status_t ntt_plan_set_small_kernel(ntt_plan_t* p, int kind) {
     if (!p) return fail(NTT_ERR_INVALID_ARGUMENT, "NULL plan");
     if (kind != NTT_SMALL_WARP && kind != NTT_SMALL_SHARED)
@@ -998,7 +1011,8 @@ ntt_status_t ntt_multiply_many(const ntt_plan_t* p, const uint32_t* a, uint32_t*
         return fail(NTT_ERR_INVALID_ARGUMENT, "plan was created on device %d, current is %d",
                     p->device, dev);
     const cudaStream_t cs = (cudaStream_t)s;
-    if (p->cfg_fwd->split) return launch_split_mul(p->cfg_fwd, p, a, b, polys, stride, cs);
+    if (p->cfg_fwd->split && p->multiply_form == NTT_MULTIPLY_ONE_LAUNCH)
+        return launch_split_mul(p->cfg_fwd, p, a, b, polys, stride, cs);
     const FusedConfig* cf =
         (polys == 1 || polys < (size_t)p->cfg_fwd->np) ? p->cfg_fwd1 : p->cfg_fwd;
     const FusedConfig* ci =

@@ -172,3 +172,30 @@ def test_multiply_spectrum_schoolbook_and_errors(torch_cuda, nb, mixes):
         p.multiply_spectrum_many(spec.data_ptr() + 4, b, 1)
     assert e.value.name == "NTT_ERR_MISALIGNED"
     p.close()
+
+
+@pytest.mark.parametrize("logN", [15, 16, 17])
+def test_multiply_forms_on_split_plans(torch_cuda, nb, mixes, logN):
+    """Both forms of ntt_multiply_many on split plans (one launch; split
+    forward, cluster forward with the product, split inverse) equal the
+    unfused calls, and the factor a is only read."""
+    torch = torch_cuda
+    pairs, limbs = 3, 4
+    mods = list(mixes.prime_pool(logN, 30, limbs))
+    a, b = pair_inputs(torch, mixes, nb, logN, mods, pairs, 90 + logN)
+    a_h = host(a).copy()
+    ref = nb.Plan(logN, mods)
+    expect = unfused(ref, a, b, pairs)
+    for form in (nb.MULTIPLY_ONE_LAUNCH, nb.MULTIPLY_THREE_LAUNCHES):
+        p = nb.Plan(logN, mods)
+        p.set_multiply_form(form)
+        x = b.clone()
+        p.multiply_many(a, x, pairs)
+        torch.cuda.synchronize()
+        assert torch.equal(x, expect), form
+        assert np.array_equal(host(a), a_h)
+        p.close()
+    with pytest.raises(nb.NttError) as e:
+        ref.set_multiply_form(5)
+    assert e.value.name == "NTT_ERR_INVALID_ARGUMENT"
+    ref.close()
