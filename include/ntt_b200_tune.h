@@ -56,7 +56,12 @@ NTT_API int ntt_config_resident_clusters(int index, int forward, int schedule);
  * phase split is requested. */
 NTT_API ntt_status_t ntt_autotune(int logN, int limbs, int polys, int iters,
                                   ntt_tune_result_t* out);
-/* Pin a plan to compiled configurations (indices into the catalogue above;
+/* The setters below (ntt_plan_force_config, ntt_plan_set_schedule,
+ * ntt_plan_set_small_kernel, ntt_plan_set_multiply_form) change how later
+ * calls on the plan launch; call them before the plan is shared between
+ * threads, not while another thread launches through it.
+ *
+ * Pin a plan to compiled configurations (indices into the catalogue above;
  * -1 keeps the current choice).  A tuning / debugging hook: results are
  * identical for every configuration. */
 NTT_API ntt_status_t ntt_plan_force_config(ntt_plan_t* plan, int fwd_index, int inv_index);

@@ -279,7 +279,9 @@ def find_moduli(logN: int, count: int, lower_bound: int) -> List[ModulusConfig]:
 
 class Plan:
     """Validated moduli + device-resident twiddle tables for one (logN,
-    modulus chain).  Immutable after creation; usable from several host
+    modulus chain).  Immutable after creation apart from the tuning setters
+    (set_schedule, set_small_kernel, set_multiply_form, force_config: call
+    them before sharing the plan); usable from several host
     threads on different streams."""
 
     def __init__(self, logN: int, moduli: Sequence, transform: Optional[TransformConfig] = None,
