@@ -7,10 +7,11 @@
 // so q < 2^62.  The Montgomery factor R = 2^64 and N^{-1} ride on the
 // stage-0 twiddle pair (table entries 0 and 1), as in the 32-bit tables.
 //
-// Kernel: one stage-range kernel.  A CTA loads G sub-transforms of 2^k
-// words of a limb into shared memory (G adjacent columns of the 2^k x
-// 2^(n-k) limb matrix for the column stages, or G adjacent rows for the row
-// stages; both loads coalesced), runs the launch's radix-2 stages there, and
+// Kernel: one stage-range kernel per launch shape.  A CTA loads G
+// sub-transforms of 2^k words of a limb into shared memory (G adjacent
+// columns of the 2^k x 2^(n-k) limb matrix for the column stages, or G
+// adjacent rows for the row stages; both loads coalesced), runs the
+// launch's radix-2 stages there, and
 // writes the words back in place.  logN <= 12: one launch with all stages on
 // whole limbs; larger: the column stages, then the row stages.
 #include <cuda_runtime.h>
@@ -86,47 +87,55 @@ struct U64Args {
     const unsigned long long* q;
     unsigned long long stride;  // words between polynomials
     uint32_t limbs, groups;     // sub-transform groups per limb
-    int n, k, s0, s1;           // logN, log2 local size, global stages [s0, s1)
-    int col;                    // 1: column stages (stride 2^(n-k)), 0: rows
-    int G;                      // sub-transforms per CTA
+    int n;                      // logN
 };
 
-// Global word offset (within the limb) of local word u of sub-transform c.
-__device__ __forceinline__ uint32_t u64_off(const U64Args& a, uint32_t c, uint32_t u) {
-    return a.col ? c + (u << (a.n - a.k)) : (c << a.k) + u;
-}
+constexpr int kU64Threads = 256;
 
-// Shared-memory index of local word u of sub-transform g (the layout the
-// coalesced loads and stores below use).
-__device__ __forceinline__ uint32_t u64_si(const U64Args& a, uint32_t g, uint32_t u) {
-    return a.col ? u * (uint32_t)a.G + g : (g << a.k) + u;
-}
+// Geometry of one stage-range launch: a CTA holds 2^GL sub-transforms of 2^K
+// words, G adjacent columns of the 2^K x 2^(n-K) limb matrix (COL) or G
+// adjacent rows, in shared memory at si(g, u).  Compile-time, so that the
+// index arithmetic of the passes is shifts and masks.
+template <int K_, int GL_, bool COL_>
+struct U64Geo {
+    static constexpr int K = K_, GL = GL_;
+    static constexpr bool COL = COL_;
+    static constexpr uint32_t KW = 1u << K, G = 1u << GL, TOTAL = KW << GL;
+    static_assert(TOTAL <= 4096, "32 KB of shared memory per CTA");
+    __device__ static __forceinline__ uint32_t si(uint32_t g, uint32_t u) {
+        return COL ? (u << GL) + g : (g << K) + u;
+    }
+    // global word offset (within the limb) of local word u of sub-transform c
+    __device__ static __forceinline__ uint32_t off(int n, uint32_t c, uint32_t u) {
+        return COL ? c + (u << (n - K)) : (c << K) + u;
+    }
+};
 
-// One register pass over local bits [bmin, bmin + RP) of every sub-transform
+// One register pass over local bits [BMIN, BMIN + RP) of every sub-transform
 // the CTA holds: a thread takes 2^RP words whose local indices differ only in
 // those bits, runs the RP stages on them in registers (forward: from the
 // highest bit down; inverse: from the lowest up) and writes them back.
-template <int RP, bool Fwd>
-__device__ __forceinline__ void u64_pass(const U64Args& a, unsigned long long* s, uint32_t c0,
-                                         int bmin, const TwPair64* tw, uint64_t q) {
+template <class Gm, int RP, int BMIN, bool Fwd>
+__device__ __forceinline__ void u64_pass(int n, unsigned long long* s, uint32_t c0,
+                                         const TwPair64* tw, uint64_t q) {
     constexpr int W = 1 << RP;
+    constexpr uint32_t rest = Gm::KW >> RP;  // local indices per group outside the pass's bits
+    constexpr uint32_t groups = Gm::G * rest;
     const uint64_t q2 = 2 * q;
-    const uint32_t K = 1u << a.k, G = (uint32_t)a.G;
-    const uint32_t rest = K >> RP;  // local indices per group outside the pass's bits
-    const uint32_t groups = G * rest;
-    for (uint32_t grp = threadIdx.x; grp < groups; grp += blockDim.x) {
+#pragma unroll 1
+    for (uint32_t grp = threadIdx.x; grp < groups; grp += kU64Threads) {
         // consecutive threads: consecutive shared-memory words where possible
-        const uint32_t g = a.col ? grp % G : grp / rest;
-        const uint32_t ur = a.col ? grp / G : grp % rest;
-        const uint32_t ubase = ((ur >> bmin) << (bmin + RP)) | (ur & ((1u << bmin) - 1u));
+        const uint32_t g = Gm::COL ? grp % Gm::G : grp / rest;
+        const uint32_t ur = Gm::COL ? grp / Gm::G : grp % rest;
+        const uint32_t ubase = ((ur >> BMIN) << (BMIN + RP)) | (ur & ((1u << BMIN) - 1u));
         uint64_t v[W];
 #pragma unroll
-        for (int j = 0; j < W; ++j) v[j] = s[u64_si(a, g, ubase | ((uint32_t)j << bmin))];
+        for (int j = 0; j < W; ++j) v[j] = s[Gm::si(g, ubase | ((uint32_t)j << BMIN))];
 #pragma unroll
         for (int t = 0; t < RP; ++t) {
             const int rb = Fwd ? RP - 1 - t : t;  // pass bit of this stage
-            const int b = bmin + rb;              // local bit
-            const int sg = a.col ? a.k - 1 - b : a.n - 1 - b;  // global stage
+            const int b = BMIN + rb;              // local bit
+            const int sg = Gm::COL ? Gm::K - 1 - b : n - 1 - b;  // global stage
             // the pair (j, j | 2^rb) sits at global distance 2^(n-1-sg), so its
             // twiddle depends only on the pass bits above rb: block h of
             // 2^rb pairs shares one, fetched with one 16-byte load just
@@ -136,9 +145,9 @@ __device__ __forceinline__ void u64_pass(const U64Args& a, unsigned long long* s
                 TwPair64 wh{0, 0};
                 if (sg != 0) {
                     const uint32_t gi =
-                        u64_off(a, c0 + g, ubase | ((uint32_t)(h << (rb + 1)) << bmin));
+                        Gm::off(n, c0 + g, ubase | ((uint32_t)(h << (rb + 1)) << BMIN));
                     const ulonglong2 p = __ldg(
-                        reinterpret_cast<const ulonglong2*>(tw + (1u << sg) + (gi >> (a.n - sg))));
+                        reinterpret_cast<const ulonglong2*>(tw + (1u << sg) + (gi >> (n - sg))));
                     wh = TwPair64{p.x, p.y};
                 }
 #pragma unroll
@@ -171,80 +180,98 @@ __device__ __forceinline__ void u64_pass(const U64Args& a, unsigned long long* s
             }
         }
 #pragma unroll
-        for (int j = 0; j < W; ++j) s[u64_si(a, g, ubase | ((uint32_t)j << bmin))] = v[j];
-    }
-}
-
-template <bool Fwd, int RPMAX>
-__device__ __forceinline__ void u64_pass_rp(int rp, const U64Args& a, unsigned long long* s,
-                                            uint32_t c0, int bmin, const TwPair64* tw,
-                                            uint64_t q) {
-    switch (rp) {
-        case 1: u64_pass<1, Fwd>(a, s, c0, bmin, tw, q); break;
-        case 2: u64_pass<2, Fwd>(a, s, c0, bmin, tw, q); break;
-        case 3: u64_pass<3, Fwd>(a, s, c0, bmin, tw, q); break;
-        default:
-            if constexpr (RPMAX >= 4) u64_pass<4, Fwd>(a, s, c0, bmin, tw, q);
-            break;
+        for (int j = 0; j < W; ++j) s[Gm::si(g, ubase | ((uint32_t)j << BMIN))] = v[j];
     }
 }
 
 // Stages per register pass (8 words per thread at 3).  Measured on B200 at
 // 2^16 x 16 limbs x 16 polynomials, forward / inverse per launch pair:
 // four-stage passes 0.66 / 0.71 ms (124 registers, 2 CTAs per SM), three-stage
-// ones 0.50 / 0.45 ms, and 0.435 / 0.453 ms with the 4-CTA launch bound below
-// (64 registers).
+// ones 0.50 / 0.45 ms, 0.435 / 0.453 ms with the 4-CTA launch bound below
+// (64 registers), and 0.371 / 0.357 ms with the launch shape compile-time.
 constexpr int kU64PassStages = 3;
 
-// Stages [s0, s1) of the CTA's sub-transforms (every local bit of them: the
-// launches of run64 give each CTA whole column or row sub-transforms), in
-// register passes of up to kU64PassStages stages with one barrier between
-// passes.
-template <bool Fwd>
-__global__ void __launch_bounds__(256, 4) u64_stage_kernel(U64Args a) {
+// The passes after the first DONE local bits: forward from the highest bit
+// down, inverse from the lowest up, kU64PassStages bits at a time, one
+// barrier after each.
+template <class Gm, bool Fwd, int DONE>
+__device__ __forceinline__ void u64_passes(int n, unsigned long long* s, uint32_t c0,
+                                           const TwPair64* tw, uint64_t q) {
+    if constexpr (DONE < Gm::K) {
+        constexpr int RP = Gm::K - DONE < kU64PassStages ? Gm::K - DONE : kU64PassStages;
+        constexpr int BMIN = Fwd ? Gm::K - DONE - RP : DONE;
+        u64_pass<Gm, RP, BMIN, Fwd>(n, s, c0, tw, q);
+        __syncthreads();
+        u64_passes<Gm, Fwd, DONE + RP>(n, s, c0, tw, q);
+    }
+}
+
+// Every local stage of the CTA's sub-transforms (the launches of run64 give
+// each CTA whole column or row sub-transforms).  LAST: the launch holds the
+// limb's last stages (the forward then stores canonical words).
+template <class Gm, bool Fwd, bool LAST>
+__global__ void __launch_bounds__(kU64Threads, 4) u64_stage_kernel(U64Args a) {
     extern __shared__ unsigned long long s[];
     const uint32_t group = blockIdx.x % a.groups;
     const uint32_t lp = blockIdx.x / a.groups;  // limb-major: limb * polys + poly
     const uint32_t polys = gridDim.x / (a.groups * a.limbs);
     const uint32_t limb = lp / polys, poly = lp - limb * polys;
-    unsigned long long* x = a.data + poly * a.stride + ((size_t)limb << a.n);
-    const TwPair64* tw = a.tw + ((size_t)limb << a.n);
+    const int n = a.n;
+    unsigned long long* x = a.data + poly * a.stride + ((size_t)limb << n);
+    const TwPair64* tw = a.tw + ((size_t)limb << n);
     const uint64_t q = a.q[limb], q2 = 2 * q;
-    const uint32_t K = 1u << a.k, G = (uint32_t)a.G, total = G * K;
-    const uint32_t c0 = group * G;
+    const uint32_t c0 = group << Gm::GL;
     // load: consecutive indices are consecutive words in global memory
-    for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
-        uint32_t g, u;
-        if (a.col) { u = i / G; g = i - u * G; }
-        else { g = i >> a.k; u = i & (K - 1); }
-        s[i] = x[u64_off(a, c0 + g, u)];
+    for (uint32_t i = threadIdx.x; i < Gm::TOTAL; i += kU64Threads) {
+        const uint32_t g = Gm::COL ? i % Gm::G : i >> Gm::K;
+        const uint32_t u = Gm::COL ? i >> Gm::GL : i % Gm::KW;
+        s[i] = x[Gm::off(n, c0 + g, u)];
     }
     __syncthreads();
-    constexpr int R = kU64PassStages;
-    if (Fwd) {
-        for (int hi = a.k; hi > 0;) {
-            const int rp = hi < R ? hi : R;
-            u64_pass_rp<true, R>(rp, a, s, c0, hi - rp, tw, q);
-            hi -= rp;
-            __syncthreads();
-        }
-    } else {
-        for (int lo = 0; lo < a.k;) {
-            const int rp = a.k - lo < R ? a.k - lo : R;
-            u64_pass_rp<false, R>(rp, a, s, c0, lo, tw, q);
-            lo += rp;
-            __syncthreads();
-        }
-    }
-    const bool canon = Fwd && a.s1 == a.n;  // the forward's last stage: canonical words
-    for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
-        uint32_t g, u;
-        if (a.col) { u = i / G; g = i - u * G; }
-        else { g = i >> a.k; u = i & (K - 1); }
+    u64_passes<Gm, Fwd, 0>(n, s, c0, tw, q);
+    for (uint32_t i = threadIdx.x; i < Gm::TOTAL; i += kU64Threads) {
+        const uint32_t g = Gm::COL ? i % Gm::G : i >> Gm::K;
+        const uint32_t u = Gm::COL ? i >> Gm::GL : i % Gm::KW;
         uint64_t v = s[i];
-        if (canon) v = csub64(csub64(v, q2), q);
-        x[u64_off(a, c0 + g, u)] = v;
+        if (Fwd && LAST) v = csub64(csub64(v, q2), q);  // canonical words
+        x[Gm::off(n, c0 + g, u)] = v;
     }
+}
+
+using U64Kernel = void (*)(U64Args);
+
+// The compiled launch shapes: logN <= 12, one launch of whole limbs
+// (K = logN, one per CTA); logN 13..17, the column stages on K1 = logN / 2
+// bits, then the row stages on K2 = logN - K1 bits, 4096 words per CTA.
+template <bool Fwd>
+U64Kernel u64_whole_kernel(int k) {
+    switch (k) {
+#define NTTB_U64_WHOLE(K) \
+    case K: return u64_stage_kernel<U64Geo<K, 0, false>, Fwd, true>;
+        NTTB_U64_WHOLE(1) NTTB_U64_WHOLE(2) NTTB_U64_WHOLE(3) NTTB_U64_WHOLE(4)
+        NTTB_U64_WHOLE(5) NTTB_U64_WHOLE(6) NTTB_U64_WHOLE(7) NTTB_U64_WHOLE(8)
+        NTTB_U64_WHOLE(9) NTTB_U64_WHOLE(10) NTTB_U64_WHOLE(11) NTTB_U64_WHOLE(12)
+#undef NTTB_U64_WHOLE
+    }
+    return nullptr;
+}
+template <bool Fwd>
+U64Kernel u64_col_kernel(int k) {  // the first stages: forward launch 1
+    switch (k) {
+        case 6: return u64_stage_kernel<U64Geo<6, 6, true>, Fwd, !Fwd>;
+        case 7: return u64_stage_kernel<U64Geo<7, 5, true>, Fwd, !Fwd>;
+        case 8: return u64_stage_kernel<U64Geo<8, 4, true>, Fwd, !Fwd>;
+    }
+    return nullptr;
+}
+template <bool Fwd>
+U64Kernel u64_row_kernel(int k) {  // the last stages: forward launch 2
+    switch (k) {
+        case 7: return u64_stage_kernel<U64Geo<7, 5, false>, Fwd, Fwd>;
+        case 8: return u64_stage_kernel<U64Geo<8, 4, false>, Fwd, Fwd>;
+        case 9: return u64_stage_kernel<U64Geo<9, 3, false>, Fwd, Fwd>;
+    }
+    return nullptr;
 }
 
 }  // namespace
@@ -313,35 +340,34 @@ ntt_status_t run64(const ntt64_plan* p, uint64_t* a, size_t polys, size_t stride
     if (dev != p->device)
         return fail(NTT_ERR_INVALID_ARGUMENT, "plan was created on device %d, current is %d",
                     p->device, dev);
-    U64Args base{(unsigned long long*)a, fwd ? p->fwd : p->inv, p->q,
-                 (unsigned long long)stride, (uint32_t)p->limbs, 1, n, n, 0, n, 0, 1};
-    std::vector<U64Args> launches;
+    const U64Args base{(unsigned long long*)a, fwd ? p->fwd : p->inv, p->q,
+                       (unsigned long long)stride, (uint32_t)p->limbs, 1, n};
+    struct Launch {
+        U64Kernel k;
+        uint32_t groups, words;  // CTAs per limb, words per CTA
+    };
+    Launch launches[2];
+    int count = 0;
     if (n <= 12) {
-        launches.push_back(base);
+        launches[count++] = {fwd ? u64_whole_kernel<true>(n) : u64_whole_kernel<false>(n), 1,
+                             1u << n};
     } else {
-        const int k1 = n / 2, k2 = n - k1;
-        U64Args c = base, r = base;
-        c.col = 1;
-        c.k = k1;
-        c.s0 = 0;
-        c.s1 = k1;
-        c.G = std::min(1 << (n - k1), 4096 >> k1);
-        c.groups = (1u << (n - k1)) / c.G;
-        r.col = 0;
-        r.k = k2;
-        r.s0 = k1;
-        r.s1 = n;
-        r.G = 4096 >> k2;
-        r.groups = (1u << k1) / r.G;
-        if (fwd) launches = {c, r};
-        else launches = {r, c};
+        const int k1 = n / 2, k2 = n - k1;  // column bits, row bits
+        const Launch c{fwd ? u64_col_kernel<true>(k1) : u64_col_kernel<false>(k1),
+                       1u << (n - 12), 4096};
+        const Launch r{fwd ? u64_row_kernel<true>(k2) : u64_row_kernel<false>(k2),
+                       1u << (n - 12), 4096};
+        launches[count++] = fwd ? c : r;
+        launches[count++] = fwd ? r : c;
     }
-    for (const U64Args& L : launches) {
+    for (int i = 0; i < count; ++i) {
+        const Launch& L = launches[i];
+        if (!L.k) return fail(NTT_ERR_UNSUPPORTED, "no 64-bit kernel for logN %d", n);
         const size_t blocks = (size_t)L.groups * p->limbs * polys;
         if (blocks > (size_t)INT_MAX) return fail(NTT_ERR_INVALID_ARGUMENT, "too many limbs");
-        const size_t smem = ((size_t)L.G << L.k) * 8;
-        if (fwd) u64_stage_kernel<true><<<(unsigned)blocks, 256, smem, s>>>(L);
-        else u64_stage_kernel<false><<<(unsigned)blocks, 256, smem, s>>>(L);
+        U64Args args = base;
+        args.groups = L.groups;
+        L.k<<<(unsigned)blocks, kU64Threads, (size_t)L.words * 8, s>>>(args);
         if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return cuda_fail(e, "64-bit NTT launch");
     }
     return NTT_OK;

@@ -26,13 +26,17 @@ def host64(t):
 
 @pytest.mark.parametrize("logN,limbs,polys,start", [
     (1, 2, 1, 1 << 59), (5, 3, 2, 1 << 60), (12, 4, 3, (1 << 61) + 7),
-    (13, 2, 2, 1 << 59), (16, 3, 2, 1 << 61), (17, 2, 1, 3 << 60)])
+    (13, 2, 2, 1 << 59), (16, 3, 2, 1 << 61), (17, 2, 1, 3 << 60)] + [
+    # every other compiled launch shape (whole limbs up to 2^12, then the
+    # column and row launches of 2^13..2^17), one limb near 2^61
+    (n, 1, 2, (1 << 61) + 3 * n) for n in (2, 3, 4, 6, 7, 8, 9, 10, 11, 14, 15)])
 def test_u64_bit_exact(torch_cuda, logN, limbs, polys, start):
     torch = torch_cuda
     import ntt_b200 as nb
     mods = [tuple(m) for m in nb.find_moduli64(logN, limbs, start)]
     T = O.LimbTables64(logN, mods)
     x = rand64(T, logN * 11 + limbs, polys)
+    x[0, 0, :2] = [T.q[0] - 1, 0]  # the largest canonical word and zero
     d = dev64(torch, x)
     with nb.Plan64(logN, mods) as p:
         p.forward_many(d, polys)
