@@ -95,15 +95,21 @@ constexpr int kU64Threads = 256;
 // Geometry of one stage-range launch: a CTA holds 2^GL sub-transforms of 2^K
 // words, G adjacent columns of the 2^K x 2^(n-K) limb matrix (COL) or G
 // adjacent rows, in shared memory at si(g, u).  Compile-time, so that the
-// index arithmetic of the passes is shifts and masks.
+// index arithmetic of the passes is shifts and masks.  Rows keep each
+// sub-transform contiguous with bits 0..3 of the word index XORed with bits
+// 4..7 (a bijection on the 2^K words): the passes over low bits would
+// otherwise put 4 to 8 threads of a half-warp on one 8-byte bank; swizzled,
+// every pass of K <= 12 has at most 2 (measured before it: 8.5 M bank
+// conflicts per row launch at 2^16 x 16 limbs x 16 polynomials).
 template <int K_, int GL_, bool COL_>
 struct U64Geo {
     static constexpr int K = K_, GL = GL_;
     static constexpr bool COL = COL_;
     static constexpr uint32_t KW = 1u << K, G = 1u << GL, TOTAL = KW << GL;
+    static constexpr bool kWholeOrCol = COL || GL == 0;  // GL == 0 only for whole limbs
     static_assert(TOTAL <= 4096, "32 KB of shared memory per CTA");
     __device__ static __forceinline__ uint32_t si(uint32_t g, uint32_t u) {
-        return COL ? (u << GL) + g : (g << K) + u;
+        return COL ? (u << GL) + g : (g << K) + (u ^ ((u >> 4) & 15u));
     }
     // global word offset (within the limb) of local word u of sub-transform c
     __device__ static __forceinline__ uint32_t off(int n, uint32_t c, uint32_t u) {
@@ -135,7 +141,9 @@ __device__ __forceinline__ void u64_pass(int n, unsigned long long* s, uint32_t 
         for (int t = 0; t < RP; ++t) {
             const int rb = Fwd ? RP - 1 - t : t;  // pass bit of this stage
             const int b = BMIN + rb;              // local bit
-            const int sg = Gm::COL ? Gm::K - 1 - b : n - 1 - b;  // global stage
+            // global stage: compile-time for the columns and for whole limbs
+            // (K = logN); row launches (logN >= 13) never hold stage 0
+            const int sg = Gm::kWholeOrCol ? Gm::K - 1 - b : n - 1 - b;
             // the pair (j, j | 2^rb) sits at global distance 2^(n-1-sg), so its
             // twiddle depends only on the pass bits above rb: block h of
             // 2^rb pairs shares one, fetched with one 16-byte load just
@@ -143,7 +151,7 @@ __device__ __forceinline__ void u64_pass(int n, unsigned long long* s, uint32_t 
 #pragma unroll
             for (int h = 0; h < (W >> (rb + 1)); ++h) {
                 TwPair64 wh{0, 0};
-                if (sg != 0) {
+                if (!Gm::kWholeOrCol || sg != 0) {
                     const uint32_t gi =
                         Gm::off(n, c0 + g, ubase | ((uint32_t)(h << (rb + 1)) << BMIN));
                     const ulonglong2 p = __ldg(
@@ -154,7 +162,7 @@ __device__ __forceinline__ void u64_pass(int n, unsigned long long* s, uint32_t 
                 for (int lo = 0; lo < (1 << rb); ++lo) {
                     const int j = (h << (rb + 1)) | lo;
                     uint64_t X = v[j], Y = v[j | (1 << rb)];
-                    if (sg == 0) {
+                    if (Gm::kWholeOrCol && sg == 0) {
                         const TwPair64 f = tw[0], fw = tw[1];
                         if (Fwd) {
                             const uint64_t A = shoup64(X, f, q), T = shoup64(Y, fw, q);
@@ -188,7 +196,8 @@ __device__ __forceinline__ void u64_pass(int n, unsigned long long* s, uint32_t 
 // 2^16 x 16 limbs x 16 polynomials, forward / inverse per launch pair:
 // four-stage passes 0.66 / 0.71 ms (124 registers, 2 CTAs per SM), three-stage
 // ones 0.50 / 0.45 ms, 0.435 / 0.453 ms with the 4-CTA launch bound below
-// (64 registers), and 0.371 / 0.357 ms with the launch shape compile-time.
+// (64 registers), 0.371 / 0.357 ms with the launch shape compile-time, and
+// 0.336 / 0.331 ms with the row swizzle and the compile-time stage index.
 constexpr int kU64PassStages = 3;
 
 // The passes after the first DONE local bits: forward from the highest bit
@@ -225,14 +234,14 @@ __global__ void __launch_bounds__(kU64Threads, 4) u64_stage_kernel(U64Args a) {
     for (uint32_t i = threadIdx.x; i < Gm::TOTAL; i += kU64Threads) {
         const uint32_t g = Gm::COL ? i % Gm::G : i >> Gm::K;
         const uint32_t u = Gm::COL ? i >> Gm::GL : i % Gm::KW;
-        s[i] = x[Gm::off(n, c0 + g, u)];
+        s[Gm::si(g, u)] = x[Gm::off(n, c0 + g, u)];
     }
     __syncthreads();
     u64_passes<Gm, Fwd, 0>(n, s, c0, tw, q);
     for (uint32_t i = threadIdx.x; i < Gm::TOTAL; i += kU64Threads) {
         const uint32_t g = Gm::COL ? i % Gm::G : i >> Gm::K;
         const uint32_t u = Gm::COL ? i >> Gm::GL : i % Gm::KW;
-        uint64_t v = s[i];
+        uint64_t v = s[Gm::si(g, u)];
         if (Fwd && LAST) v = csub64(csub64(v, q2), q);  // canonical words
         x[Gm::off(n, c0 + g, u)] = v;
     }
