@@ -93,7 +93,12 @@ typedef enum ntt_status {
 } ntt_status_t;
 
 typedef struct ntt_plan ntt_plan_t;
-typedef void* ntt_stream_t; /* cudaStream_t; NULL = legacy default stream */
+/* cudaStream_t; NULL = legacy default stream.  Calls run in stream order.
+ * Transform launches of logN <= 16 use programmatic dependent launch: one may
+ * be scheduled while the stream's previous kernel drains, but it touches no
+ * memory before that kernel has completed, so the caller's own kernels in
+ * the stream need nothing of it. */
+typedef void* ntt_stream_t;
 
 NTT_API int ntt_version(void);
 NTT_API const char* ntt_status_string(ntt_status_t status);

@@ -136,6 +136,20 @@ __device__ __forceinline__ void cluster_arrive_relaxed() {
 __device__ __forceinline__ void cluster_wait_acquire() {
     asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
+// Programmatic dependent launch: launch_fused gives the transform launches
+// of logN <= 16 cudaLaunchAttributeProgrammaticStreamSerialization, so a
+// launch may be scheduled while the kernel before it in the stream drains
+// (without the attribute both instructions below return at once).  The kernel
+// waits there for that kernel's completion (and its memory) before it
+// touches global memory, then lets the next launch be scheduled: its CTAs
+// start on the SM slots this grid leaves and wait the same way.
+__device__ __forceinline__ void pdl_enter() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
 __device__ __forceinline__ void mbar_init(uint32_t sa, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa), "r"(count) : "memory");
 }
@@ -436,6 +450,7 @@ template <class G, bool Fwd, bool Staged, class Arith, bool Mul = false, bool Su
 __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) fused_kernel(FusedArgs a) {
     static_assert(!Mul || (Fwd && !Staged), "the product epilogue follows a direct forward");
     static_assert(!Sub || (Fwd && !Staged && !Mul), "the subtract-and-scale output follows a direct forward");
+    pdl_enter();
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t rank = (G::C > 1) ? cluster_rank() : 0u;
     const uint32_t cluster = blockIdx.x / G::C;

@@ -118,6 +118,7 @@ __global__ void __launch_bounds__(G::THREADS, G::MIN_BLOCKS) split_kernel(FusedA
     static_assert(Out == kOutPlain || Fwd, "the output modes follow a forward");
     static_assert(!Comp || G::LOGN >= kTwCompMinLogN, "compressed tables start at logN 15");
     constexpr uint32_t kTwStride = Comp ? tw_comp_entries(G::LOGN) : (1u << G::LOGN);
+    pdl_enter();
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t rank = cluster_rank();
     const uint32_t cluster = blockIdx.x / G::C;
