@@ -351,6 +351,15 @@ def run_ours(args):
             plan.inverse(v, sh)
     per_call_ms = device_time(torch, stream, per_call_step, max(3, K // 100), 3)
     per_call_ms = max_over_ranks(per_call_ms)
+    # host time to submit one step's calls (the stream is idle at the start,
+    # and 2P launches stay far below the launch queue's depth, so nothing
+    # blocks): when it reaches the device time per launch, the per-call
+    # figure is the host's submission rate, not the kernels'
+    torch.cuda.synchronize()
+    t_host = time.perf_counter()
+    per_call_step()
+    host_us_per_launch = (time.perf_counter() - t_host) * 1e6 / (2 * P)
+    torch.cuda.synchronize()
 
     transforms = 2 * P * LIMBS * K * world
     value = transforms / (elapsed_max / 1000.0)
@@ -401,7 +410,10 @@ def run_ours(args):
         "gpu_launches": 2 * K,
         "per_call": {"value": 2 * P * LIMBS * world / (per_call_ms / 1000.0), "unit": "limb-NTT/s",
                      "ms_per_step": per_call_ms, "launches_per_step": 2 * P,
-                     "form": "one ntt_forward + one ntt_inverse call per polynomial"},
+                     "device_us_per_launch": per_call_ms * 1000.0 / (2 * P),
+                     "host_us_per_launch": host_us_per_launch,
+                     "form": "one ntt_forward + one ntt_inverse call per polynomial "
+                             "(Python through ctypes)"},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src,
@@ -459,6 +471,8 @@ def summary(out):
          "inverse_ms": r(out["roofline"]["inverse_ms"], 4)}
     if "per_call" in out:
         s["per_call_value"] = r(out["per_call"]["value"], 1)
+        s["per_call_us_per_launch_device_host"] = [r(out["per_call"]["device_us_per_launch"]),
+                                                   r(out["per_call"]["host_us_per_launch"])]
     if "batched" in out:
         s["batched_value"] = r(out["batched"]["value"], 1)
         s["batched_speedup_vs_plain"] = r(out["batched"]["speedup_vs_plain"])

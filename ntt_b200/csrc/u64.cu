@@ -196,8 +196,9 @@ __device__ __forceinline__ void u64_pass(int n, unsigned long long* s, uint32_t 
 // 2^16 x 16 limbs x 16 polynomials, forward / inverse per launch pair:
 // four-stage passes 0.66 / 0.71 ms (124 registers, 2 CTAs per SM), three-stage
 // ones 0.50 / 0.45 ms, 0.435 / 0.453 ms with the 4-CTA launch bound below
-// (64 registers), 0.371 / 0.357 ms with the launch shape compile-time, and
-// 0.336 / 0.331 ms with the row swizzle and the compile-time stage index.
+// (64 registers), 0.371 / 0.357 ms with the launch shape compile-time,
+// 0.336 / 0.331 ms with the row swizzle and the compile-time stage index,
+// and 0.331 / 0.326 ms with programmatic dependent launch.
 constexpr int kU64PassStages = 3;
 
 // The passes after the first DONE local bits: forward from the highest bit
@@ -220,6 +221,12 @@ __device__ __forceinline__ void u64_passes(int n, unsigned long long* s, uint32_
 // limb's last stages (the forward then stores canonical words).
 template <class Gm, bool Fwd, bool LAST>
 __global__ void __launch_bounds__(kU64Threads, 4) u64_stage_kernel(U64Args a) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+    // programmatic dependent launch (run64): wait for the stream's previous
+    // kernel before touching memory, then let the next launch be scheduled
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
     extern __shared__ unsigned long long s[];
     const uint32_t group = blockIdx.x % a.groups;
     const uint32_t lp = blockIdx.x / a.groups;  // limb-major: limb * polys + poly
@@ -376,8 +383,21 @@ ntt_status_t run64(const ntt64_plan* p, uint64_t* a, size_t polys, size_t stride
         if (blocks > (size_t)INT_MAX) return fail(NTT_ERR_INVALID_ARGUMENT, "too many limbs");
         U64Args args = base;
         args.groups = L.groups;
-        L.k<<<(unsigned)blocks, kU64Threads, (size_t)L.words * 8, s>>>(args);
-        if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return cuda_fail(e, "64-bit NTT launch");
+        // programmatic dependent launch: the row launch (and the next call's
+        // first launch) is scheduled while its predecessor drains
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3((unsigned)blocks, 1, 1);
+        lc.blockDim = dim3(kU64Threads, 1, 1);
+        lc.dynamicSmemBytes = (size_t)L.words * 8;
+        lc.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        void* kargs[] = {&args};
+        if (cudaError_t e = cudaLaunchKernelExC(&lc, (const void*)L.k, kargs); e != cudaSuccess)
+            return cuda_fail(e, "64-bit NTT launch");
     }
     return NTT_OK;
 }
