@@ -267,8 +267,9 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule) {
 // memory, the hardware scheduling the clusters.  NTT_SCHEDULE_STAGED: one
 // wave of resident clusters, each running a contiguous chunk of limb-major
 // jobs with the next input slab bulk-copied ahead.
-// Largest logN whose transform launches carry programmatic dependent launch.
-constexpr int kPdlMaxLogN = 16;
+// Largest logN whose cluster-kernel launches carry programmatic dependent
+// launch (split launches always do).
+constexpr int kPdlClusterMaxLogN = 16;
 
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
                           int schedule, bool lazy2, KernelVariant v) {
@@ -294,15 +295,16 @@ ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cu
     lc.dynamicSmemBytes = smem_of(c, schedule);
     lc.stream = s;
     // programmatic dependent launch: the kernels wait for the stream's
-    // previous kernel before touching global memory (pdl_enter), so this
+    // previous kernel before touching global memory (pdl_wait), so this
     // launch's scheduling overlaps that kernel's tail.  Measured on B200, one
     // polynomial of 16 limbs per call, forward + inverse: 2^15 13.1 against
     // 16.5 us, 2^16 17.4 against 20.8 us, 2^16 x 32 limbs 24.5 against
-    // 28.7 us, batches of 64 at 2^16 unchanged; at 2^17 39-40 against 34 us,
-    // so logN 17 launches go without it.
+    // 28.7 us, 2^17 (split, trigger after the phase exchange) 31.3 against
+    // 35.2 us; batches of 64 at 2^16 unchanged.  Cluster launches of logN 17
+    // (unmeasured) go without it.
     cudaLaunchAttribute attr[2];
     unsigned na = 0;
-    if (c->logN <= kPdlMaxLogN) {
+    if (c->split || c->logN <= kPdlClusterMaxLogN) {
         attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
         attr[na++].val.programmaticStreamSerializationAllowed = 1;
     }
