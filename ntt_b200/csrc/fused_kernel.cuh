@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "ntt_core.cuh"
+#include "pdl.cuh"
 
 namespace nttb {
 
@@ -136,29 +137,6 @@ __device__ __forceinline__ void cluster_arrive_relaxed() {
 __device__ __forceinline__ void cluster_wait_acquire() {
     asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
-// Programmatic dependent launch: launch_fused gives the split launches and
-// the cluster launches of logN <= 16 cudaLaunchAttributeProgrammaticStreamSerialization,
-// so a launch may be scheduled while the kernel before it in the stream
-// drains (without the attribute both instructions return at once).  A kernel
-// waits there for that kernel's completion (and its memory) before it
-// touches global memory (pdl_wait), and lets the next launch be scheduled
-// (pdl_trigger): its CTAs take the SM slots this grid leaves and wait the
-// same way.
-__device__ __forceinline__ void pdl_wait() {
-#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-#endif
-}
-__device__ __forceinline__ void pdl_trigger() {
-#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-#endif
-}
-__device__ __forceinline__ void pdl_enter() {
-    pdl_wait();
-    pdl_trigger();
-}
-
 __device__ __forceinline__ void mbar_init(uint32_t sa, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa), "r"(count) : "memory");
 }

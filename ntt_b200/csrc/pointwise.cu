@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include "arith.cuh"
+#include "pdl.cuh"
 #include "pointwise.h"
 
 namespace nttb {
@@ -17,6 +18,7 @@ __global__ void __launch_bounds__(256) pointwise_kernel(uint32_t* c, const uint3
                                                         const uint32_t* b, const uint32_t* q,
                                                         uint32_t limbs, uint32_t logn,
                                                         uint32_t rows, unsigned long long stride) {
+    pdl_enter();
     const uint32_t vecs = (1u << logn) >> 2;
     for (uint32_t row = blockIdx.y; row < rows; row += gridDim.y) {
         const uint32_t poly = row / limbs, limb = row - poly * limbs;
@@ -46,9 +48,8 @@ cudaError_t launch_pointwise(uint32_t* c, const uint32_t* a, const uint32_t* b,
     const uint32_t vecs = (1u << logN) >> 2;
     const uint32_t bx = (vecs + 255) / 256 < 16 ? (vecs + 255) / 256 : 16;
     const uint32_t by = rows < 65535 ? (uint32_t)rows : 65535u;
-    pointwise_kernel<<<dim3(bx, by), 256, 0, s>>>(c, a, b, q, (uint32_t)limbs, (uint32_t)logN,
-                                                  (uint32_t)rows, stride);
-    return cudaGetLastError();
+    return launch_pdl(pointwise_kernel, dim3(bx, by), dim3(256), 0, s, c, a, b, q,
+                      (uint32_t)limbs, (uint32_t)logN, (uint32_t)rows, stride);
 }
 
 }  // namespace nttb

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/ntt_b200_u64.h"
+#include "pdl.cuh"
 #include "runtime.h"
 
 using namespace nttb;
@@ -221,12 +222,7 @@ __device__ __forceinline__ void u64_passes(int n, unsigned long long* s, uint32_
 // limb's last stages (the forward then stores canonical words).
 template <class Gm, bool Fwd, bool LAST>
 __global__ void __launch_bounds__(kU64Threads, 4) u64_stage_kernel(U64Args a) {
-#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
-    // programmatic dependent launch (run64): wait for the stream's previous
-    // kernel before touching memory, then let the next launch be scheduled
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-#endif
+    pdl_enter();  // launched with programmatic dependent launch (run64)
     extern __shared__ unsigned long long s[];
     const uint32_t group = blockIdx.x % a.groups;
     const uint32_t lp = blockIdx.x / a.groups;  // limb-major: limb * polys + poly
@@ -385,18 +381,9 @@ ntt_status_t run64(const ntt64_plan* p, uint64_t* a, size_t polys, size_t stride
         args.groups = L.groups;
         // programmatic dependent launch: the row launch (and the next call's
         // first launch) is scheduled while its predecessor drains
-        cudaLaunchConfig_t lc = {};
-        lc.gridDim = dim3((unsigned)blocks, 1, 1);
-        lc.blockDim = dim3(kU64Threads, 1, 1);
-        lc.dynamicSmemBytes = (size_t)L.words * 8;
-        lc.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        lc.attrs = attr;
-        lc.numAttrs = 1;
-        void* kargs[] = {&args};
-        if (cudaError_t e = cudaLaunchKernelExC(&lc, (const void*)L.k, kargs); e != cudaSuccess)
+        if (cudaError_t e = launch_pdl(L.k, dim3((unsigned)blocks), dim3(kU64Threads),
+                                       (size_t)L.words * 8, s, args);
+            e != cudaSuccess)
             return cuda_fail(e, "64-bit NTT launch");
     }
     return NTT_OK;

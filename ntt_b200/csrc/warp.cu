@@ -24,6 +24,7 @@
 #include <utility>
 
 #include "arith.cuh"
+#include "pdl.cuh"
 #include "small.h"
 
 namespace nttb {
@@ -110,6 +111,7 @@ __device__ __forceinline__ void warp_body(uint32_t* a, const TwPair* __restrict_
 
 template <int LOGN, bool Fwd>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) warp_kernel(SmallArgs p) {
+    pdl_enter();  // launched with programmatic dependent launch (launch_warp_n)
     const uint32_t job = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     if (job >= p.jobs) return;  // uniform per warp: the shuffles see all 32 lanes
     const uint32_t jl = job % p.limbs, poly = job / p.limbs;
@@ -139,9 +141,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) warp_kernel(SmallArgs p) 
 template <int LOGN>
 cudaError_t launch_warp_n(const SmallArgs& a, bool fwd, cudaStream_t s) {
     const dim3 block(32 * kWarpsPerBlock), grid((a.jobs + kWarpsPerBlock - 1) / kWarpsPerBlock);
-    if (fwd) warp_kernel<LOGN, true><<<grid, block, 0, s>>>(a);
-    else warp_kernel<LOGN, false><<<grid, block, 0, s>>>(a);
-    return cudaGetLastError();
+    return fwd ? launch_pdl(warp_kernel<LOGN, true>, grid, block, 0, s, a)
+               : launch_pdl(warp_kernel<LOGN, false>, grid, block, 0, s, a);
 }
 
 }  // namespace
