@@ -4,7 +4,6 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "arith.cuh"
-#include "pdl.cuh"
 #include "small.h"
 
 namespace nttb {
@@ -61,7 +60,6 @@ __device__ void small_body(uint32_t* a, const TwPair* tw, uint32_t q, int logN, 
 
 template <bool Fwd>
 __global__ void small_kernel(SmallArgs p) {
-    pdl_enter();  // launched with programmatic dependent launch (launch_small)
     __shared__ uint32_t s[1u << kSmallMaxLogN];
     const uint32_t job = blockIdx.x;
     const uint32_t jl = job % p.limbs, poly = job / p.limbs;
@@ -93,8 +91,13 @@ cudaError_t launch_small(const SmallArgs& a, bool fwd, cudaStream_t s) {
     if (a.jobs == 0) return cudaSuccess;
     const uint32_t half = 1u << (a.logN - 1);
     dim3 block(half < 32 ? 32 : half), grid(a.jobs);
-    return fwd ? launch_pdl(small_kernel<true>, grid, block, 0, s, a)
-               : launch_pdl(small_kernel<false>, grid, block, 0, s, a);
+    // a plain launch: with programmatic dependent launch (waiting at the
+    // start, the trigger at the start or at the end) a batch of 2048 x 16
+    // limbs at logN 2 / 4 took 69-73 us per forward + inverse against 41-44
+    // us without it on B200, for 9.2 against 10.2 us on one-polynomial calls
+    if (fwd) small_kernel<true><<<grid, block, 0, s>>>(a);
+    else small_kernel<false><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
 }
 
 }  // namespace nttb
