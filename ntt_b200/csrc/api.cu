@@ -300,8 +300,10 @@ ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cu
     // polynomial of 16 limbs per call, forward + inverse: 2^15 13.1 against
     // 16.5 us, 2^16 17.4 against 20.8 us, 2^16 x 32 limbs 24.5 against
     // 28.7 us, 2^17 (split, trigger after the phase exchange) 31.3 against
-    // 35.2 us; batches of 64 at 2^16 unchanged.  Cluster launches of logN 17
-    // (unmeasured) go without it.
+    // 35.2 us; batches of 64 at 2^16 unchanged; cluster kernels, 16 limbs:
+    // one-polynomial calls at 2^12 10.7 against 15.4 us, 2^14 21.0 against
+    // 24.6 us, batches at 2^10 / 2^12 / 2^14 3-5% faster.  Cluster launches of
+    // logN 17 (unmeasured) go without it.
     cudaLaunchAttribute attr[2];
     unsigned na = 0;
     if (c->split || c->logN <= kPdlClusterMaxLogN) {
