@@ -94,8 +94,8 @@ typedef enum ntt_status {
 
 typedef struct ntt_plan ntt_plan_t;
 /* cudaStream_t; NULL = legacy default stream.  Calls run in stream order.
- * The launches of the transforms (except the cluster kernels at logN 17 and
- * the small kernel of logN <= 5), of ntt_pointwise_mul and of the 64-bit
+ * The launches of the transforms (except the small kernel of logN <= 5), of
+ * ntt_pointwise_mul and of the 64-bit
  * variant use programmatic dependent launch: one may be scheduled while the
  * stream's previous kernel drains, but it touches no memory before that
  * kernel has completed, so the caller's own kernels in the stream need

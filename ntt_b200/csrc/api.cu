@@ -267,10 +267,6 @@ int config_resident_clusters(const FusedConfig* c, bool fwd, int schedule) {
 // memory, the hardware scheduling the clusters.  NTT_SCHEDULE_STAGED: one
 // wave of resident clusters, each running a contiguous chunk of limb-major
 // jobs with the next input slab bulk-copied ahead.
-// Largest logN whose cluster-kernel launches carry programmatic dependent
-// launch (split launches always do).
-constexpr int kPdlClusterMaxLogN = 16;
-
 ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cudaStream_t s,
                           int schedule, bool lazy2, KernelVariant v) {
     if (a.jobs == 0) return NTT_OK;
@@ -302,14 +298,12 @@ ntt_status_t launch_fused(const FusedConfig* c, bool fwd, const FusedArgs& a, cu
     // 28.7 us, 2^17 (split, trigger after the phase exchange) 31.3 against
     // 35.2 us; batches of 64 at 2^16 unchanged; cluster kernels, 16 limbs:
     // one-polynomial calls at 2^12 10.7 against 15.4 us, 2^14 21.0 against
-    // 24.6 us, batches at 2^10 / 2^12 / 2^14 3-5% faster.  Cluster launches of
-    // logN 17 (unmeasured) go without it.
+    // 24.6 us, at 2^17 3-8%, batches at 2^10 / 2^12 / 2^14 3-5% faster, the
+    // product at 2^17 (split, cluster with the product, split) 0.5-1%.
     cudaLaunchAttribute attr[2];
     unsigned na = 0;
-    if (c->split || c->logN <= kPdlClusterMaxLogN) {
-        attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[na++].val.programmaticStreamSerializationAllowed = 1;
-    }
+    attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[na++].val.programmaticStreamSerializationAllowed = 1;
     if (C > 1) {
         attr[na].id = cudaLaunchAttributeClusterDimension;
         attr[na].val.clusterDim.x = C;

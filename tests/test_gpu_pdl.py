@@ -2,10 +2,10 @@
 
 Transform launches carry programmatic dependent launch (the split kernels,
 which trigger the next launch at their start up to logN 16 and after the
-phase exchange at logN 17, and the cluster kernels up to logN 16): such a
-launch may be scheduled while the kernel before it in the stream drains, and
-the kernel waits for that one's completion before it touches memory
-(pdl_wait in fused_kernel.cuh).  These chains feed each launch's output to the next, mix
+phase exchange at logN 17, and the cluster kernels): such a launch may be
+scheduled while the kernel before it in the stream drains, and the kernel
+waits for that one's completion before it touches memory (pdl_wait in
+pdl.cuh).  These chains feed each launch's output to the next, mix
 in torch kernels (launched without the attribute) that read and rewrite the
 buffers, and compare with the oracle and with the same chain synchronised
 after every call.  Needs a B200.
